@@ -1,0 +1,383 @@
+/*
+ * ref_harness.c -- TEST INFRASTRUCTURE ONLY (oracle).
+ *
+ * Drives the reference's own, unmodified gravity sources (compiled from the
+ * reference tree by oracle/ref/Makefile against single-rank stub headers) for
+ * one short-range force computation and dumps every intermediate that the
+ * B200 library must reproduce:
+ *
+ *   domain_Decomposition()            domain/domain.c:78-185
+ *     -> Peano-Hilbert keys + sort      domain/domain_toplevel.c:120-135, domain/peano.c:74-133
+ *     -> top-level tree                 domain/domain_toplevel.c:111-269
+ *   construct_forcetree(0, 1, 0, bin) gravity/forcetree.c:110-149     (as gravity/accel.c:127-132)
+ *   force_treeevaluate() per target   gravity/forcetree_walk.c:115-514 (per-target acc, pot, interactions)
+ *   gravity_tree(bin)                 gravity/gravtree.c:357-707       (cross-check of GravAccel)
+ *   gravity_force_finalize(bin)       gravity/accel.c:204-347          (OldAcc for the relative pass)
+ *
+ * and then repeats build + walk with the relative opening criterion, exactly
+ * as compute_grav_accelerations() does on the first step (gravity/accel.c:58-80).
+ *
+ * Usage: ref_harness <in.bin> <out.bin> [key=value ...]
+ *   in.bin  : int64 N, then N*3 double positions, N double masses, N uint8 softening types
+ *   keys    : box, asmth, rcut (periodic build only), theta, erracc, eps0, eps1 (Plummer
+ *             softening per type), mdom (MultipleDomains), tnf (TopNodeFactor),
+ *             passes (1 = BH only, 2 = BH then relative), dump (1 = write tree),
+ *             stride (walk every stride-th particle in the timed loop), first, count
+ *             (walk a contiguous slice of sorted targets; used for CPU timing),
+ *             gt (1 = also run gravity_tree), tag (string printed with timings)
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/time.h>
+
+#include "allvars.h"
+#include "proto.h"
+#include "../domain/domain.h"
+
+static double wall(void)
+{
+  struct timeval tv;
+  gettimeofday(&tv, NULL);
+  return tv.tv_sec + 1e-6 * tv.tv_usec;
+}
+
+static double arg_d(int argc, char **argv, const char *key, double def)
+{
+  size_t l = strlen(key);
+  for(int i = 3; i < argc; i++)
+    if(strncmp(argv[i], key, l) == 0 && argv[i][l] == '=')
+      return atof(argv[i] + l + 1);
+  return def;
+}
+
+static void wr(FILE *f, const void *p, size_t sz, size_t n)
+{
+  if(n && fwrite(p, sz, n, f) != n)
+    {
+      fprintf(stderr, "ref_harness: short write\n");
+      exit(2);
+    }
+}
+
+static void wsec(FILE *f, const char *name, int64_t nbytes)
+{
+  char tag[16];
+  memset(tag, 0, sizeof(tag));
+  strncpy(tag, name, 15);
+  wr(f, tag, 1, 16);
+  wr(f, &nbytes, 8, 1);
+}
+
+static void split_key(peanokey k, uint64_t *hi, uint64_t *lo)
+{
+  unsigned __int128 u = (unsigned __int128)k;
+  *lo                 = (uint64_t)u;
+  *hi                 = (uint64_t)(u >> 64);
+}
+
+/* walk the selected sorted targets with the reference's per-target routine */
+static double walk_targets(int first, int count, int stride, double *acc, double *pot, int *ninter)
+{
+  double t0 = wall();
+  for(int i = first; i < first + count; i += stride)
+    {
+      gravdata_in in;
+      gravdata_out out;
+      for(int k = 0; k < 3; k++)
+        in.Pos[k] = P[i].Pos[k];
+      in.Type          = P[i].Type;
+      in.SofteningType = P[i].SofteningType;
+      in.OldAcc        = P[i].OldAcc;
+      in.Firstnode     = 0;
+      int n            = force_treeevaluate(&in, &out, i, 0, 0, 1, NULL, 0);
+      if(acc)
+        {
+          for(int k = 0; k < 3; k++)
+            acc[3 * i + k] = out.Acc[k];
+          pot[i]    = out.Potential;
+          ninter[i] = n;
+        }
+    }
+  return wall() - t0;
+}
+
+static void dump_tree(FILE *f)
+{
+  int nn = Tree_NumNodes;
+  wsec(f, "tree_meta", 6 * 8);
+  int64_t meta[6] = {Tree_MaxPart, Tree_MaxNodes, nn, Tree_FirstNonTopLevelNode, NTopnodes, NTopleaves};
+  wr(f, meta, 8, 6);
+  /* nodes in index order [Tree_MaxPart, Tree_MaxPart + nn) */
+  wsec(f, "node_f64", (int64_t)nn * 8 * 8);
+  for(int no = Tree_MaxPart; no < Tree_MaxPart + nn; no++)
+    {
+      double v[8] = {Nodes[no].center[0], Nodes[no].center[1], Nodes[no].center[2], Nodes[no].len,
+                     Nodes[no].u.d.s[0],  Nodes[no].u.d.s[1],  Nodes[no].u.d.s[2],  Nodes[no].u.d.mass};
+      wr(f, v, 8, 8);
+    }
+  wsec(f, "node_i32", (int64_t)nn * 4 * 4);
+  for(int no = Tree_MaxPart; no < Tree_MaxPart + nn; no++)
+    {
+      int32_t v[4] = {Nodes[no].u.d.sibling, Nodes[no].u.d.nextnode, Nodes[no].u.d.father, Nodes[no].u.d.maxsofttype};
+      wr(f, v, 4, 4);
+    }
+  wsec(f, "nextnode", (int64_t)NumPart * 4);
+  wr(f, Nextnode, 4, NumPart);
+  wsec(f, "father", (int64_t)NumPart * 4);
+  wr(f, Father, 4, NumPart);
+}
+
+static void free_tree(void)
+{
+  /* same release sequence as gravity() (gravity/accel.c:153-156) */
+  myfree(Father);
+  myfree(Nextnode);
+  myfree(Tree_Points);
+  force_treefree();
+}
+
+int main(int argc, char **argv)
+{
+  if(argc < 3)
+    {
+      fprintf(stderr, "usage: %s in.bin out.bin [key=value ...]\n", argv[0]);
+      return 1;
+    }
+
+  ThisTask = 0;
+  NTask    = 1;
+  for(PTask = 0; NTask > (1 << PTask); PTask++)
+    ;
+
+  FILE *fi = fopen(argv[1], "rb");
+  if(!fi)
+    {
+      fprintf(stderr, "cannot open %s\n", argv[1]);
+      return 1;
+    }
+  int64_t n64;
+  if(fread(&n64, 8, 1, fi) != 1)
+    return 1;
+  int n          = (int)n64;
+  double *pos    = malloc(sizeof(double) * 3 * n);
+  double *mass   = malloc(sizeof(double) * n);
+  uint8_t *stype = malloc(n);
+  if(fread(pos, 8, 3 * (size_t)n, fi) != 3 * (size_t)n || fread(mass, 8, n, fi) != (size_t)n || fread(stype, 1, n, fi) != (size_t)n)
+    {
+      fprintf(stderr, "short input\n");
+      return 1;
+    }
+  fclose(fi);
+
+  int passes = (int)arg_d(argc, argv, "passes", 2);
+  int dump   = (int)arg_d(argc, argv, "dump", 1);
+  int stride = (int)arg_d(argc, argv, "stride", 1);
+  int first  = (int)arg_d(argc, argv, "first", 0);
+  int count  = (int)arg_d(argc, argv, "count", n);
+  int run_gt = (int)arg_d(argc, argv, "gt", 1);
+  if(first < 0 || first > n)
+    first = 0;
+  if(count < 0 || first + count > n)
+    count = n - first;
+  if(stride < 1)
+    stride = 1;
+
+  /* ---- run parameters (what read_parameter_file + init would set) ---- */
+  All.BoxSize                = arg_d(argc, argv, "box", 1.0);
+  All.ErrTolTheta            = arg_d(argc, argv, "theta", 0.7);
+  All.ErrTolForceAcc         = arg_d(argc, argv, "erracc", 0.0025);
+  All.TypeOfOpeningCriterion = 1;
+  All.ComovingIntegrationOn  = 0;
+  All.G                      = 1.0;
+  All.MultipleDomains        = (int)arg_d(argc, argv, "mdom", 8);
+  All.TopNodeFactor          = arg_d(argc, argv, "tnf", 2.5);
+  All.TopNodeAllocFactor     = 0.08;
+  All.TreeAllocFactor        = 0.7;
+  if(n < 1000)
+    All.TreeAllocFactor = 10.0; /* init/init.c */
+  All.SofteningComoving[0] = arg_d(argc, argv, "eps0", 0.01);
+  All.SofteningComoving[1] = arg_d(argc, argv, "eps1", 0.01);
+  All.SofteningMaxPhys[0]  = All.SofteningComoving[0];
+  All.SofteningMaxPhys[1]  = All.SofteningComoving[1];
+  All.MaxPart              = n;
+  All.MaxPartSph           = 0;
+  All.TotNumPart           = n;
+  All.TotNumGas            = 0;
+  All.Ti_Current           = 0;
+  All.Time                 = 1.0;
+  All.TimeBegin            = 0.0;
+  All.TimeMax              = 1.0;
+  All.ActivePartFracForNewDomainDecomp = 0.01;
+  size_t need_mb = (size_t)(((double)n * 1400.0) / (1024.0 * 1024.0)) + 512;
+  All.MaxMemSize = (int)need_mb;
+  boxSize        = All.BoxSize;
+  boxHalf        = 0.5 * All.BoxSize;
+
+  /* the log files the reference writes to (io/logs.c:70-213) go to /dev/null */
+  FdInfo = FdEnergy = FdTimings = FdDomain = FdBalance = FdMemory = FdTimebin = FdCPU = fopen("/dev/null", "w");
+
+  mymalloc_init();
+  timebins_init(&TimeBinsHydro, "Hydro", &All.MaxPartSph);
+  timebins_init(&TimeBinsGravity, "Gravity", &All.MaxPart);
+  NumPart = n;
+  NumGas  = 0;
+  allocate_memory();
+
+  for(int i = 0; i < GRAVCOSTLEVELS; i++)
+    All.LevelToTimeBin[i] = -1;
+
+  for(int i = 0; i < n; i++)
+    {
+      memset(&P[i], 0, sizeof(struct particle_data));
+      for(int k = 0; k < 3; k++)
+        P[i].Pos[k] = pos[3 * i + k];
+      P[i].Mass          = mass[i];
+      P[i].Type          = 1;
+      P[i].SofteningType = stype[i];
+      P[i].ID            = (MyIDType)(i + 1);
+      P[i].TimeBinGrav   = 0;
+      P[i].TimeBinHydro  = 0;
+      P[i].Ti_Current    = 0;
+      P[i].OldAcc        = 0;
+    }
+  for(int i = 0; i < TIMEBINS; i++)
+    TimeBinSynchronized[i] = 1;
+  reconstruct_timebins();
+  mark_active_timebins();
+
+  set_softenings();
+  force_short_range_init();
+#ifdef PMGRID
+  All.Asmth[0] = arg_d(argc, argv, "asmth", 1.25 / PMGRID);
+  All.Rcut[0]  = arg_d(argc, argv, "rcut", RCUT * All.Asmth[0]);
+#endif
+
+  double t0 = wall();
+  domain_Decomposition();
+  double t_domain = wall() - t0;
+
+  int bin   = All.HighestActiveTimeBin;
+  FILE *fo  = fopen(argv[2], "wb");
+  if(!fo)
+    return 1;
+  wr(fo, "GGREFOUT", 1, 8);
+
+  wsec(fo, "domain", 10 * 8);
+  double dom[10] = {DomainCorner[0], DomainCorner[1], DomainCorner[2], DomainCenter[0], DomainCenter[1],
+                    DomainCenter[2], DomainLen,       DomainInverseLen, DomainBigFac,   (double)NTopnodes};
+  wr(fo, dom, 8, 10);
+
+  wsec(fo, "order", (int64_t)n * 8);
+  for(int i = 0; i < n; i++)
+    {
+      int64_t o = (int64_t)P[i].ID - 1;
+      wr(fo, &o, 8, 1);
+    }
+  wsec(fo, "keys", (int64_t)n * 16);
+  for(int i = 0; i < n; i++)
+    {
+      peano1D xb = domain_double_to_int(((P[i].Pos[0] - DomainCorner[0]) * DomainInverseLen) + 1.0);
+      peano1D yb = domain_double_to_int(((P[i].Pos[1] - DomainCorner[1]) * DomainInverseLen) + 1.0);
+      peano1D zb = domain_double_to_int(((P[i].Pos[2] - DomainCorner[2]) * DomainInverseLen) + 1.0);
+      uint64_t kk[2];
+      split_key(peano_hilbert_key(xb, yb, zb, BITS_PER_DIMENSION), &kk[0], &kk[1]);
+      wr(fo, kk, 8, 2);
+    }
+  wsec(fo, "topnodes", (int64_t)NTopnodes * 48);
+  for(int i = 0; i < NTopnodes; i++)
+    {
+      uint64_t k[4];
+      split_key(TopNodes[i].StartKey, &k[0], &k[1]);
+      split_key(TopNodes[i].Size, &k[2], &k[3]);
+      wr(fo, k, 8, 4);
+      int32_t dl[2] = {TopNodes[i].Daughter, TopNodes[i].Leaf};
+      wr(fo, dl, 4, 2);
+      wr(fo, TopNodes[i].MortonToPeanoSubnode, 1, 8);
+    }
+
+  double *acc  = malloc(sizeof(double) * 3 * n);
+  double *pot  = malloc(sizeof(double) * n);
+  int *ninter  = malloc(sizeof(int) * n);
+  double *gacc = malloc(sizeof(double) * 3 * n);
+
+  for(int pass = 0; pass < passes; pass++)
+    {
+      double tb0 = wall();
+      construct_forcetree(0, 1, 0, bin);
+      double t_build = wall() - tb0;
+
+      if(dump && pass == 0)
+        dump_tree(fo);
+
+      memset(acc, 0, sizeof(double) * 3 * n);
+      memset(pot, 0, sizeof(double) * n);
+      memset(ninter, 0, sizeof(int) * n);
+      double t_walk = walk_targets(first, count, stride, acc, pot, ninter);
+
+      double t_gt = 0;
+      if(run_gt)
+        {
+          double tg0 = wall();
+          gravity_tree(bin);
+          t_gt = wall() - tg0;
+          for(int i = 0; i < n; i++)
+            for(int k = 0; k < 3; k++)
+              gacc[3 * i + k] = P[i].GravAccel[k];
+        }
+      else if(All.TypeOfOpeningCriterion == 1)
+        All.ErrTolTheta = 0; /* what gravity_tree() does at its end (gravity/gravtree.c:654-655) */
+
+      char nm[16];
+      snprintf(nm, sizeof(nm), "acc%d", pass);
+      wsec(fo, nm, (int64_t)n * 24);
+      wr(fo, acc, 8, 3 * (size_t)n);
+      snprintf(nm, sizeof(nm), "pot%d", pass);
+      wsec(fo, nm, (int64_t)n * 8);
+      wr(fo, pot, 8, n);
+      snprintf(nm, sizeof(nm), "ninter%d", pass);
+      wsec(fo, nm, (int64_t)n * 4);
+      wr(fo, ninter, 4, n);
+      if(run_gt)
+        {
+          snprintf(nm, sizeof(nm), "gacc%d", pass);
+          wsec(fo, nm, (int64_t)n * 24);
+          wr(fo, gacc, 8, 3 * (size_t)n);
+        }
+
+      if(!run_gt)
+        {
+          /* store the walk results where gravity_tree() would have put them */
+          for(int i = 0; i < n; i++)
+            for(int k = 0; k < 3; k++)
+              P[i].GravAccel[k] = acc[3 * i + k];
+        }
+      gravity_force_finalize(bin);
+      free_tree();
+
+      snprintf(nm, sizeof(nm), "oldacc%d", pass);
+      wsec(fo, nm, (int64_t)n * 4);
+      for(int i = 0; i < n; i++)
+        {
+          float oa = P[i].OldAcc;
+          wr(fo, &oa, 4, 1);
+        }
+
+      long long nint = 0;
+      int nt         = 0;
+      for(int i = first; i < first + count; i += stride)
+        nint += ninter[i], nt++;
+      snprintf(nm, sizeof(nm), "time%d", pass);
+      wsec(fo, nm, 6 * 8);
+      double tv[6] = {t_domain, t_build, t_walk, t_gt, (double)nt, (double)nint};
+      wr(fo, tv, 8, 6);
+      printf("pass=%d N=%d domain=%.6f build=%.6f walk=%.6f (targets=%d, interactions=%lld) gravity_tree=%.6f\n", pass, n,
+             t_domain, t_build, t_walk, nt, nint, t_gt);
+    }
+
+  wsec(fo, "end", 0);
+  fclose(fo);
+  return 0;
+}
