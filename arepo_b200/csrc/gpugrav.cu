@@ -1,0 +1,734 @@
+// gpugrav.cu -- C ABI of libarepo_gpugrav: context, call sequencing, transfers.
+//
+// The call sequence mirrors gravity() (src/gravity/accel.c:94-192) on one rank:
+//   gpugrav_load   ~ do_box_wrapping + domain_findExtent + keys + peano_hilbert_order
+//   gpugrav_build  ~ construct_forcetree(0, ...)
+//   gpugrav_walk   ~ gravity_tree(timebin)
+// Errors are returned as status codes (negative codes mirror force_treebuild_construct's);
+// nothing in the library exits.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "internal.h"
+
+using namespace gg;
+
+// ------------------------------------------------------------------------------
+// buffers
+// ------------------------------------------------------------------------------
+cudaError_t gg::DevBuf::ensure(size_t bytes)
+{
+  if(bytes <= cap && p)
+    return cudaSuccess;
+  if(p)
+    cudaFree(p);
+  p   = nullptr;
+  cap = 0;
+  size_t want = bytes < 256 ? 256 : bytes;
+  want        = (want + 255) & ~(size_t)255;
+  cudaError_t e = cudaMalloc(&p, want);
+  if(e != cudaSuccess)
+    {
+      p = nullptr;
+      return e;
+    }
+  cap = want;
+  return cudaSuccess;
+}
+
+void gg::DevBuf::release()
+{
+  if(p)
+    cudaFree(p);
+  p   = nullptr;
+  cap = 0;
+}
+
+cudaError_t gg::PinnedBuf::ensure(size_t bytes)
+{
+  if(bytes <= cap && p)
+    return cudaSuccess;
+  if(p)
+    cudaFreeHost(p);
+  p             = nullptr;
+  cap           = 0;
+  cudaError_t e = cudaMallocHost(&p, bytes);
+  if(e != cudaSuccess)
+    {
+      p = nullptr;
+      return e;
+    }
+  cap = bytes;
+  return cudaSuccess;
+}
+
+void gg::PinnedBuf::release()
+{
+  if(p)
+    cudaFreeHost(p);
+  p   = nullptr;
+  cap = 0;
+}
+
+// ------------------------------------------------------------------------------
+// helpers
+// ------------------------------------------------------------------------------
+namespace
+{
+int fail(gpugrav_ctx *c, int status, const char *what, cudaError_t e = cudaSuccess)
+{
+  if(c)
+    {
+      char buf[512];
+      if(e != cudaSuccess)
+        snprintf(buf, sizeof(buf), "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+      else
+        snprintf(buf, sizeof(buf), "%s", what);
+      c->err = buf;
+    }
+  return status;
+}
+
+#define CK(call, what)                                 \
+  do                                                   \
+    {                                                  \
+      cudaError_t _e = (call);                         \
+      if(_e != cudaSuccess)                            \
+        return fail(c, GPUGRAV_ERR_CUDA, what, _e);    \
+    }                                                  \
+  while(0)
+
+int validate_params(const gpugrav_params *p)
+{
+  if(!p || p->abi_version != GPUGRAV_ABI_VERSION)
+    return GPUGRAV_ERR_INVALID;
+  if(p->nsofttypes < 1 || p->nsofttypes > GPUGRAV_MAX_SOFTTYPES)
+    return GPUGRAV_ERR_INVALID;
+  if(p->force_softening[p->nsofttypes] != 0.0)
+    return GPUGRAV_ERR_INVALID;
+  for(int i = 0; i < p->nsofttypes; i++)
+    if(!(p->force_softening[i] >= 0.0) || !std::isfinite(p->force_softening[i]))
+      return GPUGRAV_ERR_INVALID;
+  if(!(p->box_size > 0) || !std::isfinite(p->box_size))
+    return GPUGRAV_ERR_INVALID;
+  if(p->periodic)
+    {
+      if(!(p->asmth > 0) || !(p->rcut > 0) || !(p->rcut_cells > 0))
+        return GPUGRAV_ERR_INVALID;
+    }
+  if(!(p->err_tol_theta >= 0) || !(p->err_tol_force_acc >= 0))
+    return GPUGRAV_ERR_INVALID;
+  if(p->precision != GPUGRAV_PREC_FP64 && p->precision != GPUGRAV_PREC_FP32)
+    return GPUGRAV_ERR_INVALID;
+  if(p->multiple_domains < 1 || p->multiple_domains > 512 || !(p->top_node_factor > 0))
+    return GPUGRAV_ERR_INVALID;
+  return GPUGRAV_OK;
+}
+
+__global__ void k_gather_f32(const float *__restrict__ in, const uint32_t *__restrict__ perm, int64_t n, float *__restrict__ out)
+{
+  for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = in ? in[perm[i]] : 0.0f;
+}
+
+__global__ void k_scatter_out(const double *__restrict__ acc_s, const double *__restrict__ pot_s, const int32_t *__restrict__ nint_s,
+                              const uint32_t *__restrict__ perm, int64_t n, double *__restrict__ acc, double *__restrict__ pot,
+                              int32_t *__restrict__ nint)
+{
+  for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    {
+      int64_t o      = perm[i];
+      acc[3 * o + 0] = acc_s[3 * i + 0];
+      acc[3 * o + 1] = acc_s[3 * i + 1];
+      acc[3 * o + 2] = acc_s[3 * i + 2];
+      if(pot)
+        pot[o] = pot_s[i];
+      if(nint)
+        nint[o] = nint_s[i];
+    }
+}
+
+int grid_for(int64_t n, int threads)
+{
+  int64_t b = (n + threads - 1) / threads;
+  if(b > 148 * 16)
+    b = 148 * 16;
+  return (int)(b < 1 ? 1 : b);
+}
+
+struct DeviceGuard
+{
+  int prev = -1;
+  explicit DeviceGuard(int dev)
+  {
+    cudaGetDevice(&prev);
+    if(prev != dev)
+      cudaSetDevice(dev);
+  }
+  ~DeviceGuard()
+  {
+    if(prev >= 0)
+      cudaSetDevice(prev);
+  }
+};
+
+float elapsed(cudaEvent_t a, cudaEvent_t b)
+{
+  float ms = 0;
+  if(cudaEventElapsedTime(&ms, a, b) != cudaSuccess)
+    return 0;
+  return ms;
+}
+}  // namespace
+
+// short-range table exactly as force_short_range_init (src/gravity/forcetree_walk.c:72-85)
+void gg::make_walk_const(const gpugrav_params &p, WalkConst *w)
+{
+  memset(w, 0, sizeof(*w));
+  w->periodic = p.periodic;
+  w->bh       = p.err_tol_theta > 0 ? 1 : 0;
+  w->box      = p.box_size;
+  w->half_box = 0.5 * p.box_size;
+  w->theta    = p.err_tol_theta;
+  w->erracc   = p.err_tol_force_acc;
+  for(int i = 0; i <= p.nsofttypes; i++)
+    w->soft[i] = p.force_softening[i];
+  if(p.periodic)
+    {
+      double rcut     = p.rcut;
+      double asmth    = p.asmth;
+      double asmthinv = 0.5 / asmth;
+      w->rcut         = rcut;
+      w->rcut2        = rcut * rcut;
+      w->asmthinv2    = asmthinv * asmthinv;
+      w->asmthfac     = asmthinv * (kNtab / (p.rcut_cells / 2.0));
+      for(int i = 0; i <= kNtab; i++)
+        {
+          double u          = ((p.rcut_cells / 2.0) / kNtab) * i;
+          w->tab_pot[i]     = (float)(-erfc(u));
+          w->tab_force[i]   = (u > 0) ? (float)((erfc(u) + 2.0 * u / sqrt(M_PI) * exp(-u * u) - 1.0) / (u * u)) : 0.0f;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------
+extern "C" {
+
+int32_t gpugrav_abi_version(void) { return GPUGRAV_ABI_VERSION; }
+
+const char *gpugrav_status_string(int32_t s)
+{
+  switch(s)
+    {
+      case GPUGRAV_OK:
+        return "ok";
+      case GPUGRAV_ERR_TREE_FULL:
+        return "tree storage exhausted (-1)";
+      case GPUGRAV_ERR_TOPNODES:
+        return "top-level nodes invalid or do not fit (-2)";
+      case GPUGRAV_ERR_OUT_OF_BOX:
+        return "particle outside the domain box (-3): redo the domain decomposition";
+      case GPUGRAV_ERR_INVALID:
+        return "invalid argument";
+      case GPUGRAV_ERR_OOM:
+        return "out of memory";
+      case GPUGRAV_ERR_CUDA:
+        return "CUDA error";
+      case GPUGRAV_ERR_TIMEOUT:
+        return "bounded wait timed out";
+      case GPUGRAV_ERR_STATE:
+        return "call order violated";
+      case GPUGRAV_ERR_DEEP_TREE:
+        return "tree deeper than supported";
+      case GPUGRAV_ERR_UNSUPPORTED:
+        return "unsupported option";
+      default:
+        return "unknown status";
+    }
+}
+
+const char *gpugrav_last_error(gpugrav_ctx *c) { return c ? c->err.c_str() : "no context"; }
+
+int32_t gpugrav_create(gpugrav_ctx **out, int32_t device, const gpugrav_params *p)
+{
+  if(!out)
+    return GPUGRAV_ERR_INVALID;
+  *out  = nullptr;
+  int v = validate_params(p);
+  if(v != GPUGRAV_OK)
+    return v;
+  int ndev = 0;
+  if(cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+    {
+      cudaGetLastError();
+      return GPUGRAV_ERR_CUDA;
+    }
+  gpugrav_ctx *c = new(std::nothrow) gpugrav_ctx();
+  if(!c)
+    return GPUGRAV_ERR_OOM;
+  c->device = device;
+  c->prm    = *p;
+  DeviceGuard g(device);
+  if(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    {
+      delete c;
+      return GPUGRAV_ERR_CUDA;
+    }
+  c->own_stream = true;
+  for(auto &e : c->ev)
+    if(cudaEventCreate(&e) != cudaSuccess)
+      {
+        delete c;
+        return GPUGRAV_ERR_CUDA;
+      }
+  if(c->bconst.ensure(sizeof(BuildConst)) != cudaSuccess || c->wconst.ensure(sizeof(WalkConst)) != cudaSuccess ||
+     c->counters.ensure(64 * sizeof(int)) != cudaSuccess)
+    {
+      delete c;
+      return GPUGRAV_ERR_OOM;
+    }
+  *out = c;
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_destroy(gpugrav_ctx *c)
+{
+  if(!c)
+    return GPUGRAV_ERR_INVALID;
+  DeviceGuard g(c->device);
+  cudaStreamSynchronize(c->stream);
+  gg::DevBuf *bufs[] = {&c->bconst, &c->wconst, &c->pos_in, &c->mass_in, &c->st_in, &c->key, &c->key_alt, &c->idx, &c->perm,
+                        &c->sort_tmp, &c->s_pm, &c->s_ix, &c->s_iy, &c->s_iz, &c->s_st, &c->s_cd, &c->s_tl, &c->s_tlnode,
+                        &c->cnt, &c->base, &c->hcnt, &c->hack_list, &c->hack_scratch, &c->counters, &c->top, &c->skel,
+                        &c->n_suns, &c->n_depth, &c->n_cl, &c->n_sm, &c->n_maxsoft, &c->n_size, &c->n_father, &c->n_sibling,
+                        &c->n_next, &c->n_dfs, &c->n_first, &c->p_next, &c->p_father, &c->p_dfs, &c->depth_hist,
+                        &c->depth_order, &c->w_sm, &c->w_cl, &c->w_link, &c->w32_a, &c->w32_b, &c->acc_s, &c->pot_s,
+                        &c->nint_s, &c->oldacc_s, &c->oldacc_in, &c->out_acc, &c->out_pot, &c->out_nint, &c->scratch};
+  for(auto *b : bufs)
+    b->release();
+  c->pinned.release();
+  for(auto &e : c->ev)
+    if(e)
+      cudaEventDestroy(e);
+  if(c->own_stream && c->stream)
+    cudaStreamDestroy(c->stream);
+  delete c;
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_set_params(gpugrav_ctx *c, const gpugrav_params *p)
+{
+  if(!c)
+    return GPUGRAV_ERR_INVALID;
+  int v = validate_params(p);
+  if(v != GPUGRAV_OK)
+    return fail(c, v, "invalid parameters");
+  bool geometry_changed = (p->periodic != c->prm.periodic) || (p->box_size != c->prm.box_size) ||
+                          (p->nsofttypes != c->prm.nsofttypes) ||
+                          memcmp(p->force_softening, c->prm.force_softening, sizeof(p->force_softening)) != 0;
+  c->prm = *p;
+  if(geometry_changed)
+    {
+      c->loaded = false;
+      c->built  = false;
+    }
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_set_stream(gpugrav_ctx *c, void *stream)
+{
+  if(!c)
+    return GPUGRAV_ERR_INVALID;
+  DeviceGuard g(c->device);
+  cudaStreamSynchronize(c->stream);
+  if(c->own_stream && c->stream)
+    cudaStreamDestroy(c->stream);
+  if(stream)
+    {
+      c->stream     = (cudaStream_t)stream;
+      c->own_stream = false;
+    }
+  else
+    {
+      if(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(c, GPUGRAV_ERR_CUDA, "stream creation");
+      c->own_stream = true;
+    }
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_synchronize(gpugrav_ctx *c)
+{
+  if(!c)
+    return GPUGRAV_ERR_INVALID;
+  DeviceGuard g(c->device);
+  CK(cudaStreamSynchronize(c->stream), "synchronize");
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_load(gpugrav_ctx *c, int64_t n, const double *pos, const double *mass, const uint8_t *softtype, int32_t mem,
+                     const gpugrav_domain *dom)
+{
+  if(!c)
+    return GPUGRAV_ERR_INVALID;
+  if(n < 2 || n >= (int64_t)1 << 30 || !pos || !mass || !softtype || (mem != GPUGRAV_MEM_HOST && mem != GPUGRAV_MEM_DEVICE))
+    return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_load: need n >= 2, n < 2^30 and non-null arrays");
+  DeviceGuard g(c->device);
+  c->loaded = false;
+  c->built  = false;
+  c->n      = n;
+  cudaStream_t st = c->stream;
+  cudaEventRecord(c->ev[0], st);
+  if(c->pos_in.ensure(n * 3 * sizeof(double)) != cudaSuccess || c->mass_in.ensure(n * sizeof(double)) != cudaSuccess ||
+     c->st_in.ensure(n + 16) != cudaSuccess)
+    return fail(c, GPUGRAV_ERR_OOM, "gpugrav_load: device allocation");
+  cudaMemcpyKind kind = (mem == GPUGRAV_MEM_HOST) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  CK(cudaMemcpyAsync(c->pos_in.p, pos, n * 3 * sizeof(double), kind, st), "upload positions");
+  CK(cudaMemcpyAsync(c->mass_in.p, mass, n * sizeof(double), kind, st), "upload masses");
+  CK(cudaMemcpyAsync(c->st_in.p, softtype, n, kind, st), "upload softening types");
+  cudaEventRecord(c->ev[1], st);
+
+  // softening types must index ForceSoftening[0..nsofttypes-1]: validated on the host copy when given
+  BuildConst bc;
+  memset(&bc, 0, sizeof(bc));
+  bc.n        = n;
+  bc.periodic = c->prm.periodic;
+  bc.nsoft    = c->prm.nsofttypes;
+  bc.box      = c->prm.box_size;
+  for(int i = 0; i <= c->prm.nsofttypes; i++)
+    bc.soft[i] = c->prm.force_softening[i];
+  if(dom)
+    {
+      if(!(dom->len > 0) || !std::isfinite(dom->len))
+        return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_load: invalid domain");
+      bc.dom = *dom;
+    }
+  CK(cudaMemcpyAsync(c->bconst.p, &bc, sizeof(bc), cudaMemcpyHostToDevice, st), "upload constants");
+
+  int flags = 0;
+  CK(gg::domain_stage(c, dom == nullptr, &flags), "domain stage");
+  if(flags & 2)
+    return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_load: non-finite particle position");
+  if(flags & 1)
+    return fail(c, GPUGRAV_ERR_OUT_OF_BOX, "gpugrav_load: particle outside the domain box");
+  cudaEventRecord(c->ev[2], st);
+  CK(gg::sort_stage(c), "key sort");
+  cudaEventRecord(c->ev[3], st);
+  CK(gg::gather_stage(c), "gather");
+  CK(cudaMemcpyAsync(&bc, c->bconst.p, sizeof(bc), cudaMemcpyDeviceToHost, st), "download domain");
+  CK(cudaMemcpyAsync(&flags, c->counters.p, sizeof(int), cudaMemcpyDeviceToHost, st), "download flags");
+  CK(cudaStreamSynchronize(st), "domain stage");
+  c->dom = bc.dom;
+  if(flags & 4)
+    return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_load: softening type >= nsofttypes");
+  c->timings.upload_ms = elapsed(c->ev[0], c->ev[1]);
+  c->timings.domain_ms = elapsed(c->ev[1], c->ev[2]);
+  c->timings.sort_ms   = elapsed(c->ev[2], c->ev[3]);
+  c->loaded            = true;
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_build(gpugrav_ctx *c, const gpugrav_topnode *top, int32_t ntop)
+{
+  if(!c)
+    return GPUGRAV_ERR_INVALID;
+  if(!c->loaded)
+    return fail(c, GPUGRAV_ERR_STATE, "gpugrav_build before gpugrav_load");
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->stream;
+  c->built        = false;
+  cudaEventRecord(c->ev[4], st);
+  if(top)
+    {
+      if(ntop < 1 || ntop > kMaxTop)
+        return fail(c, GPUGRAV_ERR_TOPNODES, "gpugrav_build: top node count out of range");
+      if(c->top.ensure(kMaxTop * sizeof(gpugrav_topnode)) != cudaSuccess)
+        return fail(c, GPUGRAV_ERR_OOM, "top nodes");
+      c->top_host.assign(top, top + ntop);
+      CK(cudaMemcpyAsync(c->top.p, top, ntop * sizeof(gpugrav_topnode), cudaMemcpyHostToDevice, st), "upload top nodes");
+      c->ntop = ntop;
+    }
+  else
+    {
+      int s = 0;
+      CK(gg::toptree_stage(c, &s), "top tree");
+      if(s != GPUGRAV_OK)
+        return fail(c, s, "gpugrav_build: top-level tree could not be refined (PEANOGRID too coarse)");
+    }
+  cudaEventRecord(c->ev[5], st);
+  int s = 0;
+  CK(gg::build_stage(c, &s), "tree build");
+  if(s != GPUGRAV_OK)
+    return fail(c, s, s == GPUGRAV_ERR_TOPNODES ? "gpugrav_build: invalid top-level tree"
+                                                : "gpugrav_build: tree build self-check failed");
+  cudaEventRecord(c->ev[6], st);
+  CK(cudaStreamSynchronize(st), "tree build");
+  c->timings.toptree_ms = elapsed(c->ev[4], c->ev[5]);
+  c->timings.build_ms   = elapsed(c->ev[5], c->ev[6]);
+  c->built              = true;
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_walk(gpugrav_ctx *c, const float *oldacc, double *acc, double *pot, int32_t *ninter, int32_t mem)
+{
+  if(!c)
+    return GPUGRAV_ERR_INVALID;
+  if(!c->built)
+    return fail(c, GPUGRAV_ERR_STATE, "gpugrav_walk before gpugrav_build");
+  if(!acc || (mem != GPUGRAV_MEM_HOST && mem != GPUGRAV_MEM_DEVICE))
+    return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_walk: acc must be non-null");
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->stream;
+  const int64_t n = c->n;
+  if(c->acc_s.ensure(n * 3 * sizeof(double)) != cudaSuccess || c->pot_s.ensure(n * sizeof(double)) != cudaSuccess ||
+     c->nint_s.ensure(n * sizeof(int32_t)) != cudaSuccess || c->oldacc_s.ensure(n * sizeof(float)) != cudaSuccess ||
+     c->oldacc_in.ensure(n * sizeof(float)) != cudaSuccess)
+    return fail(c, GPUGRAV_ERR_OOM, "gpugrav_walk: device allocation");
+  WalkConst wc;
+  make_walk_const(c->prm, &wc);
+  CK(cudaMemcpyAsync(c->wconst.p, &wc, sizeof(wc), cudaMemcpyHostToDevice, st), "walk constants");
+  cudaEventRecord(c->ev[7], st);
+  const float *old_dev = nullptr;
+  if(oldacc)
+    {
+      if(mem == GPUGRAV_MEM_HOST)
+        {
+          CK(cudaMemcpyAsync(c->oldacc_in.p, oldacc, n * sizeof(float), cudaMemcpyHostToDevice, st), "upload OldAcc");
+          old_dev = c->oldacc_in.as<float>();
+        }
+      else
+        old_dev = oldacc;
+    }
+  k_gather_f32<<<grid_for(n, 256), 256, 0, st>>>(old_dev, c->perm.as<uint32_t>(), n, c->oldacc_s.as<float>());
+  CK(cudaMemsetAsync(c->counters.as<int>() + 32, 0, 8, st), "reset counters");
+  cudaEventRecord(c->ev[8], st);
+  if(c->prm.precision == GPUGRAV_PREC_FP32)
+    {
+      CK(gg::walk32_stage(c, wc), "fp32 walk");
+    }
+  else
+    {
+      CK(gg::walk64_stage(c, wc), "fp64 walk");
+    }
+  cudaEventRecord(c->ev[9], st);
+  double *d_acc = acc, *d_pot = pot;
+  int32_t *d_nint = ninter;
+  if(mem == GPUGRAV_MEM_HOST)
+    {
+      if(c->out_acc.ensure(n * 3 * sizeof(double)) != cudaSuccess || c->out_pot.ensure(n * sizeof(double)) != cudaSuccess ||
+         c->out_nint.ensure(n * sizeof(int32_t)) != cudaSuccess)
+        return fail(c, GPUGRAV_ERR_OOM, "gpugrav_walk: output staging");
+      d_acc  = c->out_acc.as<double>();
+      d_pot  = pot ? c->out_pot.as<double>() : nullptr;
+      d_nint = ninter ? c->out_nint.as<int32_t>() : nullptr;
+    }
+  k_scatter_out<<<grid_for(n, 256), 256, 0, st>>>(c->acc_s.as<double>(), c->pot_s.as<double>(), c->nint_s.as<int32_t>(),
+                                                  c->perm.as<uint32_t>(), n, d_acc, d_pot, d_nint);
+  CK(cudaGetLastError(), "scatter");
+  if(mem == GPUGRAV_MEM_HOST)
+    {
+      CK(cudaMemcpyAsync(acc, d_acc, n * 3 * sizeof(double), cudaMemcpyDeviceToHost, st), "download acc");
+      if(pot)
+        CK(cudaMemcpyAsync(pot, d_pot, n * sizeof(double), cudaMemcpyDeviceToHost, st), "download pot");
+      if(ninter)
+        CK(cudaMemcpyAsync(ninter, d_nint, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "download interactions");
+    }
+  unsigned long long tot = 0;
+  CK(cudaMemcpyAsync(&tot, c->counters.as<int>() + 32, 8, cudaMemcpyDeviceToHost, st), "interaction total");
+  cudaEventRecord(c->ev[10], st);
+  CK(cudaStreamSynchronize(st), "walk");
+  c->timings.walk_ms              = elapsed(c->ev[8], c->ev[9]);
+  c->timings.download_ms          = elapsed(c->ev[9], c->ev[10]);
+  c->timings.interactions         = (int64_t)tot;
+  c->timings.walk_kernel_launches = 1;
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_compute(gpugrav_ctx *c, int64_t n, const double *pos, const double *mass, const uint8_t *softtype,
+                        const float *oldacc, const gpugrav_domain *dom, const gpugrav_topnode *top, int32_t ntop, double *acc,
+                        double *pot, int32_t *ninter, int32_t mem)
+{
+  int s = gpugrav_load(c, n, pos, mass, softtype, mem, dom);
+  if(s != GPUGRAV_OK)
+    return s;
+  s = gpugrav_build(c, top, ntop);
+  if(s != GPUGRAV_OK)
+    return s;
+  return gpugrav_walk(c, oldacc, acc, pot, ninter, mem);
+}
+
+int32_t gpugrav_get_domain(gpugrav_ctx *c, gpugrav_domain *dom)
+{
+  if(!c || !dom)
+    return GPUGRAV_ERR_INVALID;
+  if(!c->loaded)
+    return fail(c, GPUGRAV_ERR_STATE, "no particles loaded");
+  *dom = c->dom;
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_get_order(gpugrav_ctx *c, int64_t *order)
+{
+  if(!c || !order)
+    return GPUGRAV_ERR_INVALID;
+  if(!c->loaded)
+    return fail(c, GPUGRAV_ERR_STATE, "no particles loaded");
+  DeviceGuard g(c->device);
+  std::vector<uint32_t> tmp(c->n);
+  CK(cudaMemcpyAsync(tmp.data(), c->perm.p, c->n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream), "download order");
+  CK(cudaStreamSynchronize(c->stream), "download order");
+  for(int64_t i = 0; i < c->n; i++)
+    order[i] = tmp[i];
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_get_keys(gpugrav_ctx *c, uint64_t *hi, uint64_t *lo)
+{
+  if(!c || !hi || !lo)
+    return GPUGRAV_ERR_INVALID;
+  if(!c->loaded)
+    return fail(c, GPUGRAV_ERR_STATE, "no particles loaded");
+  DeviceGuard g(c->device);
+  std::vector<u128> tmp(c->n);
+  CK(cudaMemcpyAsync(tmp.data(), c->key_alt.p, c->n * sizeof(u128), cudaMemcpyDeviceToHost, c->stream), "download keys");
+  CK(cudaStreamSynchronize(c->stream), "download keys");
+  for(int64_t i = 0; i < c->n; i++)
+    {
+      hi[i] = (uint64_t)(tmp[i] >> 64);
+      lo[i] = (uint64_t)tmp[i];
+    }
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_get_topnodes(gpugrav_ctx *c, gpugrav_topnode *top, int32_t capacity, int32_t *ntop)
+{
+  if(!c || !ntop)
+    return GPUGRAV_ERR_INVALID;
+  if(!c->built)
+    return fail(c, GPUGRAV_ERR_STATE, "no tree built");
+  *ntop = (int32_t)c->top_host.size();
+  if(top)
+    {
+      if(capacity < *ntop)
+        return fail(c, GPUGRAV_ERR_INVALID, "top node buffer too small");
+      memcpy(top, c->top_host.data(), c->top_host.size() * sizeof(gpugrav_topnode));
+    }
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_get_tree_info(gpugrav_ctx *c, gpugrav_tree_info *info)
+{
+  if(!c || !info)
+    return GPUGRAV_ERR_INVALID;
+  if(!c->built)
+    return fail(c, GPUGRAV_ERR_STATE, "no tree built");
+  info->num_particles    = c->n;
+  info->max_part         = c->n;
+  info->num_nodes        = c->num_nodes;
+  info->first_non_top    = c->n + c->ntop;
+  info->num_topnodes     = c->ntop;
+  info->num_topleaves    = c->nleaves;
+  info->max_depth        = c->max_depth;
+  info->coincident_cells = c->hack_cells;
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_export_tree(gpugrav_ctx *c, double *center, double *len, double *s, double *mass, int32_t *sibling,
+                            int32_t *nextnode, int32_t *father, uint8_t *maxsofttype, int32_t *p_next, int32_t *p_father)
+{
+  if(!c)
+    return GPUGRAV_ERR_INVALID;
+  if(!c->built)
+    return fail(c, GPUGRAV_ERR_STATE, "no tree built");
+  DeviceGuard g(c->device);
+  const int64_t nn = c->num_nodes, n = c->n;
+  cudaStream_t st  = c->stream;
+  std::vector<double4> cl, sm;
+  if(center || len)
+    {
+      cl.resize(nn);
+      CK(cudaMemcpyAsync(cl.data(), c->n_cl.p, nn * sizeof(double4), cudaMemcpyDeviceToHost, st), "export");
+    }
+  if(s || mass)
+    {
+      sm.resize(nn);
+      CK(cudaMemcpyAsync(sm.data(), c->n_sm.p, nn * sizeof(double4), cudaMemcpyDeviceToHost, st), "export");
+    }
+  if(sibling)
+    CK(cudaMemcpyAsync(sibling, c->n_sibling.p, nn * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "export");
+  if(nextnode)
+    CK(cudaMemcpyAsync(nextnode, c->n_next.p, nn * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "export");
+  if(father)
+    CK(cudaMemcpyAsync(father, c->n_father.p, nn * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "export");
+  if(maxsofttype)
+    CK(cudaMemcpyAsync(maxsofttype, c->n_maxsoft.p, nn, cudaMemcpyDeviceToHost, st), "export");
+  if(p_next)
+    CK(cudaMemcpyAsync(p_next, c->p_next.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "export");
+  if(p_father)
+    CK(cudaMemcpyAsync(p_father, c->p_father.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "export");
+  CK(cudaStreamSynchronize(st), "export");
+  for(int64_t k = 0; k < nn; k++)
+    {
+      if(center)
+        {
+          center[3 * k + 0] = cl[k].x;
+          center[3 * k + 1] = cl[k].y;
+          center[3 * k + 2] = cl[k].z;
+        }
+      if(len)
+        len[k] = cl[k].w;
+      if(s)
+        {
+          s[3 * k + 0] = sm[k].x;
+          s[3 * k + 1] = sm[k].y;
+          s[3 * k + 2] = sm[k].z;
+        }
+      if(mass)
+        mass[k] = sm[k].w;
+    }
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_get_timings(gpugrav_ctx *c, gpugrav_timings *t)
+{
+  if(!c || !t)
+    return GPUGRAV_ERR_INVALID;
+  *t = c->timings;
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_direct(gpugrav_ctx *c, int64_t ntargets, const int64_t *targets, double *acc, double *pot)
+{
+  if(!c || ntargets < 0 || (ntargets > 0 && (!targets || !acc)))
+    return GPUGRAV_ERR_INVALID;
+  if(!c->loaded)
+    return fail(c, GPUGRAV_ERR_STATE, "gpugrav_direct before gpugrav_load");
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->stream;
+  for(int64_t i = 0; i < ntargets; i++)
+    if(targets[i] < 0 || targets[i] >= c->n)
+      return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_direct: target index out of range");
+  gg::DevBuf dt, da, dp;
+  if(dt.ensure(ntargets * 8 + 8) != cudaSuccess || da.ensure(ntargets * 24 + 8) != cudaSuccess ||
+     dp.ensure(ntargets * 8 + 8) != cudaSuccess)
+    return fail(c, GPUGRAV_ERR_OOM, "gpugrav_direct: allocation");
+  WalkConst wc;
+  make_walk_const(c->prm, &wc);
+  CK(cudaMemcpyAsync(c->wconst.p, &wc, sizeof(wc), cudaMemcpyHostToDevice, st), "walk constants");
+  CK(cudaMemcpyAsync(dt.p, targets, ntargets * 8, cudaMemcpyHostToDevice, st), "targets");
+  CK(gg::direct_stage(c, wc, ntargets, dt.as<int64_t>(), da.as<double>(), dp.as<double>()), "direct summation");
+  CK(cudaMemcpyAsync(acc, da.p, ntargets * 24, cudaMemcpyDeviceToHost, st), "download");
+  if(pot)
+    CK(cudaMemcpyAsync(pot, dp.p, ntargets * 8, cudaMemcpyDeviceToHost, st), "download");
+  CK(cudaStreamSynchronize(st), "direct summation");
+  dt.release();
+  da.release();
+  dp.release();
+  return GPUGRAV_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,138 @@
+// internal.h -- shared definitions of libarepo_gpugrav (not part of the C ABI).
+//
+// Floating point on the parity path (keys, build, moments, FP64 walk) must
+// round exactly like the reference's plain C doubles: the translation units
+// that implement it are compiled with -fmad=false, and the helpers below spell
+// out the IEEE operations where a contraction would otherwise be tempting.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/gpugrav.h"
+
+namespace gg
+{
+typedef unsigned __int128 u128;
+
+constexpr int kBits         = 42;  // BITS_PER_DIMENSION (src/main/allvars.h:370-372)
+constexpr int kMaxTreeLevel = 30;  // MAX_TREE_LEVEL (src/gravity/forcetree.h:106)
+constexpr int kNtab         = GPUGRAV_NTAB;
+constexpr int kMaxTop       = 4096;  // top-level nodes held in shared memory by the build kernels
+constexpr int32_t kNodeFlag = 1 << 8;
+
+// Per-build constants (small, read by every kernel): lives in device memory, copied to
+// registers/shared memory by the kernels.
+struct BuildConst
+{
+  gpugrav_domain dom;
+  int64_t n;         // particles
+  int32_t ntop;      // skeleton nodes (NTopnodes, root included)
+  int32_t nleaves;   // NTopleaves
+  int32_t periodic;
+  int32_t nsoft;
+  double box;
+  double soft[GPUGRAV_MAX_SOFTTYPES + 1];
+};
+
+// Walk constants
+struct WalkConst
+{
+  int32_t periodic;
+  int32_t bh;        // 1: Barnes-Hut criterion (ErrTolTheta > 0), 0: relative criterion
+  double box, half_box;
+  double theta;      // ErrTolTheta
+  double erracc;     // ErrTolForceAcc
+  double rcut, rcut2, asmthinv2, asmthfac;
+  double soft[GPUGRAV_MAX_SOFTTYPES + 1];
+  float tab_force[kNtab + 1];
+  float tab_pot[kNtab + 1];
+};
+
+// Device buffer that only grows.
+struct DevBuf
+{
+  void *p    = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes);
+  void release();
+  template <class T>
+  T *as() const
+  {
+    return (T *)p;
+  }
+};
+
+struct PinnedBuf
+{
+  void *p    = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes);
+  void release();
+};
+
+}  // namespace gg
+
+struct gpugrav_ctx
+{
+  int device            = 0;
+  cudaStream_t stream   = nullptr;
+  bool own_stream       = false;
+  gpugrav_params prm{};
+  std::string err;
+
+  // ---- state ----
+  int64_t n          = 0;
+  bool loaded        = false;
+  bool built         = false;
+  int32_t ntop       = 0;  // skeleton nodes
+  int32_t nleaves    = 0;
+  int64_t num_nodes  = 0;  // total nodes (skeleton + dynamic)
+  int64_t n_entries  = 0;  // walk entries = n + num_nodes
+  int32_t max_depth  = 0;
+  int32_t hack_cells = 0;
+  gpugrav_domain dom{};
+  std::vector<gpugrav_topnode> top_host;
+
+  // ---- device buffers ----
+  gg::DevBuf bconst, wconst;
+  gg::DevBuf pos_in, mass_in, st_in;          // caller order
+  gg::DevBuf key, key_alt, idx, perm;         // keys / sort
+  gg::DevBuf sort_tmp;
+  gg::DevBuf s_pm, s_ix, s_iy, s_iz, s_st;    // sorted SoA: (x,y,z,m) double4, 52-bit coordinates, softening type
+  gg::DevBuf s_cd, s_tl, s_tlnode;            // pair depth, top-leaf depth / node
+  gg::DevBuf cnt, base, hcnt, hack_list, hack_scratch, counters;
+  gg::DevBuf top, skel;                       // top nodes, skeleton description
+  gg::DevBuf n_suns, n_depth, n_cl, n_sm, n_maxsoft, n_size, n_father, n_sibling, n_next, n_dfs, n_first;
+  gg::DevBuf p_next, p_father, p_dfs;
+  gg::DevBuf depth_hist, depth_order;
+  gg::DevBuf w_sm, w_cl, w_link;              // walk layout (DFS order)
+  gg::DevBuf w32_a, w32_b;                    // FP32 walk layout
+  gg::DevBuf acc_s, pot_s, nint_s, oldacc_s, oldacc_in;  // per target (sorted), inputs
+  gg::DevBuf out_acc, out_pot, out_nint;      // caller order staging for host copies
+  gg::DevBuf scratch;                         // reductions
+  gg::PinnedBuf pinned;
+
+  cudaEvent_t ev[16] = {};
+  gpugrav_timings timings{};
+};
+
+namespace gg
+{
+// launchers implemented in the .cu files; each returns cudaGetLastError() of its launches
+cudaError_t domain_stage(gpugrav_ctx *c, bool compute_extent, int *out_of_box);
+cudaError_t sort_stage(gpugrav_ctx *c);
+cudaError_t gather_stage(gpugrav_ctx *c);
+cudaError_t toptree_stage(gpugrav_ctx *c, int *status);
+cudaError_t skeleton_stage(gpugrav_ctx *c, int *status);
+cudaError_t build_stage(gpugrav_ctx *c, int *status);
+cudaError_t walk64_stage(gpugrav_ctx *c, const WalkConst &wc);
+cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc);
+cudaError_t layout32_stage(gpugrav_ctx *c);
+cudaError_t direct_stage(gpugrav_ctx *c, const WalkConst &wc, int64_t nt, const int64_t *d_targets, double *d_acc,
+                         double *d_pot);
+void make_walk_const(const gpugrav_params &p, WalkConst *wc);
+}  // namespace gg

@@ -1,0 +1,185 @@
+"""Host-side interface of the B200 tree-gravity engine, shaped like the
+reference's gravity driver.
+
+    reference (src/gravity/accel.c:58-80, 94-192)        here
+    ----------------------------------------------       -------------------------------
+    domain_Decomposition()   [keys + sort part]          GravityTree.domain_decomposition()
+    construct_forcetree(0, ...)                          GravityTree.construct_forcetree()
+    gravity_tree(timebin)                                GravityTree.gravity_tree()
+    compute_grav_accelerations() on the first step       GravityTree.compute_grav_accelerations()
+      (Barnes-Hut pass, OldAcc, relative pass)
+
+Everything runs in libarepo_gpugrav on the GPU; this module only moves
+arguments across the C ABI and raises GpuGravError on a negative status (the
+reference's -1/-2/-3 codes keep their meaning).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+
+
+class GravityTree:
+    def __init__(self, params: L.Params, device: int = 0):
+        self.lib = L.load()
+        self.params = params
+        self._ctx = C.c_void_p()
+        self._check(self.lib.gpugrav_create(C.byref(self._ctx), device, C.byref(params)), ctx=False)
+        self.n = 0
+
+    # ---- lifetime ----
+    def close(self):
+        if self._ctx:
+            self.lib.gpugrav_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, status: int, ctx: bool = True):
+        if status != L.OK:
+            msg = self.lib.gpugrav_status_string(status).decode()
+            if ctx and self._ctx:
+                msg += ": " + self.lib.gpugrav_last_error(self._ctx).decode()
+            raise L.GpuGravError(status, msg)
+
+    def set_params(self, params: L.Params):
+        self._check(self.lib.gpugrav_set_params(self._ctx, C.byref(params)))
+        self.params = params
+
+    def set_stream(self, stream_handle: int | None):
+        self._check(self.lib.gpugrav_set_stream(self._ctx, C.c_void_p(stream_handle) if stream_handle else None))
+
+    def synchronize(self):
+        self._check(self.lib.gpugrav_synchronize(self._ctx))
+
+    # ---- the path ----
+    def domain_decomposition(self, pos, mass, softtype, domain: L.Domain | None = None, mem: int = L.MEM_HOST):
+        """Wrap, extent (unless `domain` is given), 126-bit keys and stable key sort.
+        Host arrays (numpy) with mem=MEM_HOST; device tensors with mem=MEM_DEVICE."""
+        if mem == L.MEM_HOST:
+            pos = np.ascontiguousarray(pos, np.float64)
+            mass = np.ascontiguousarray(mass, np.float64)
+            softtype = np.ascontiguousarray(softtype, np.uint8)
+        n = len(mass)
+        self._keep = (pos, mass, softtype)
+        self._check(
+            self.lib.gpugrav_load(
+                self._ctx, n, L.ptr(pos), L.ptr(mass), L.ptr(softtype), mem, C.byref(domain) if domain is not None else None
+            )
+        )
+        self.n = n
+
+    def construct_forcetree(self, topnodes: np.ndarray | None = None) -> int:
+        """Top-level skeleton, octree, moments, threading. Returns Tree_NumNodes."""
+        if topnodes is not None:
+            top = np.ascontiguousarray(topnodes, L.TOPNODE_DTYPE)
+            self._check(self.lib.gpugrav_build(self._ctx, top.ctypes.data_as(C.c_void_p), len(top)))
+        else:
+            self._check(self.lib.gpugrav_build(self._ctx, None, 0))
+        return self.tree_info().num_nodes
+
+    def gravity_tree(self, oldacc=None, acc=None, pot=None, ninter=None, mem: int = L.MEM_HOST):
+        """Accelerations (without G), potentials and interaction counts for every particle,
+        in the caller's order. With mem=MEM_HOST numpy outputs are allocated when not given."""
+        n = self.n
+        if mem == L.MEM_HOST:
+            if acc is None:
+                acc = np.empty((n, 3), np.float64)
+            if pot is None:
+                pot = np.empty(n, np.float64)
+            if ninter is None:
+                ninter = np.empty(n, np.int32)
+            if oldacc is not None:
+                oldacc = np.ascontiguousarray(oldacc, np.float32)
+        self._check(self.lib.gpugrav_walk(self._ctx, L.ptr(oldacc), L.ptr(acc), L.ptr(pot), L.ptr(ninter), mem))
+        return acc, pot, ninter
+
+    def compute_grav_accelerations(self, pos, mass, softtype, topnodes=None, pm_acc=None):
+        """First-step sequence of compute_grav_accelerations (src/gravity/accel.c:58-80):
+        Barnes-Hut pass, OldAcc = |a_tree + a_PM/G| (gravity_force_finalize, accel.c:237-255),
+        then the relative-criterion pass. Returns (acc, pot, ninter, oldacc) of the second pass."""
+        self.domain_decomposition(pos, mass, softtype)
+        self.construct_forcetree(topnodes)
+        p = self.params
+        theta = p.err_tol_theta
+        acc, pot, ni = self.gravity_tree()
+        a = acc if pm_acc is None else acc + pm_acc
+        oldacc = np.sqrt(a[:, 0] * a[:, 0] + a[:, 1] * a[:, 1] + a[:, 2] * a[:, 2]).astype(np.float32)
+        if p.type_of_opening_criterion == 1:
+            p.err_tol_theta = 0.0  # gravity_tree switches to the relative criterion (gravtree.c:654-655)
+            self.set_params(p)
+            try:
+                acc, pot, ni = self.gravity_tree(oldacc)
+            finally:
+                p.err_tol_theta = theta
+                self.set_params(p)
+        return acc, pot, ni, oldacc
+
+    # ---- introspection ----
+    def domain(self) -> L.Domain:
+        d = L.Domain()
+        self._check(self.lib.gpugrav_get_domain(self._ctx, C.byref(d)))
+        return d
+
+    def order(self) -> np.ndarray:
+        o = np.empty(self.n, np.int64)
+        self._check(self.lib.gpugrav_get_order(self._ctx, L.ptr(o)))
+        return o
+
+    def keys(self):
+        hi = np.empty(self.n, np.uint64)
+        lo = np.empty(self.n, np.uint64)
+        self._check(self.lib.gpugrav_get_keys(self._ctx, L.ptr(hi), L.ptr(lo)))
+        return hi, lo
+
+    def topnodes(self) -> np.ndarray:
+        nt = C.c_int32()
+        self._check(self.lib.gpugrav_get_topnodes(self._ctx, None, 0, C.byref(nt)))
+        out = np.zeros(nt.value, L.TOPNODE_DTYPE)
+        self._check(self.lib.gpugrav_get_topnodes(self._ctx, out.ctypes.data_as(C.c_void_p), nt.value, C.byref(nt)))
+        return out
+
+    def tree_info(self) -> L.TreeInfo:
+        t = L.TreeInfo()
+        self._check(self.lib.gpugrav_get_tree_info(self._ctx, C.byref(t)))
+        return t
+
+    def export_tree(self) -> dict:
+        info = self.tree_info()
+        nn, n = info.num_nodes, self.n
+        t = dict(
+            center=np.empty((nn, 3)), len=np.empty(nn), s=np.empty((nn, 3)), mass=np.empty(nn),
+            sibling=np.empty(nn, np.int32), nextnode=np.empty(nn, np.int32), father=np.empty(nn, np.int32),
+            maxsoft=np.empty(nn, np.uint8), p_next=np.empty(n, np.int32), p_father=np.empty(n, np.int32),
+        )
+        self._check(self.lib.gpugrav_export_tree(self._ctx, *[L.ptr(t[k]) for k in (
+            "center", "len", "s", "mass", "sibling", "nextnode", "father", "maxsoft", "p_next", "p_father")]))
+        t.update(num_nodes=int(nn), max_part=int(info.max_part), first_non_top=int(info.first_non_top),
+                 max_depth=int(info.max_depth), coincident_cells=int(info.coincident_cells))
+        return t
+
+    def timings(self) -> L.Timings:
+        t = L.Timings()
+        self._check(self.lib.gpugrav_get_timings(self._ctx, C.byref(t)))
+        return t
+
+    def direct(self, targets) -> tuple[np.ndarray, np.ndarray]:
+        """FP64 direct summation for the given caller indices (accuracy instrument)."""
+        tg = np.ascontiguousarray(targets, np.int64)
+        acc = np.empty((len(tg), 3))
+        pot = np.empty(len(tg))
+        self._check(self.lib.gpugrav_direct(self._ctx, len(tg), L.ptr(tg), L.ptr(acc), L.ptr(pot)))
+        return acc, pot

@@ -1,0 +1,207 @@
+/*
+ * gpugrav.h -- C ABI of libarepo_gpugrav, a B200 (sm_100a) engine for AREPO's
+ * short-range TreePM tree gravity.
+ *
+ * The library replaces the pair
+ *     construct_forcetree(0, ...);   src/gravity/forcetree.c:110-149
+ *     gravity_tree(timebin);         src/gravity/gravtree.c:357-707
+ * inside gravity() (src/gravity/accel.c:127-134), including the Peano-Hilbert
+ * key generation and key sort that precede it (src/domain/domain_toplevel.c:120-135,
+ * src/domain/peano.c:74-133).  gravity_force_finalize(), the PM long-range
+ * force, the rest of the domain decomposition and the hydro stay in the caller.
+ *
+ * Conventions (all as in the reference):
+ *   - accelerations are returned WITHOUT the factor G (gravity_force_finalize
+ *     multiplies by G, src/gravity/accel.c:258-265);
+ *   - OldAcc is a float per particle (src/main/allvars.h:1266);
+ *   - particles are addressed in the caller's order; the library sorts them
+ *     internally (stable, by 126-bit Peano-Hilbert key) and scatters results back;
+ *   - negative status codes mirror force_treebuild_construct's -1/-2/-3
+ *     (src/gravity/forcetree.c:313-318); the library never exits or aborts.
+ *
+ * Plain pointers and sizes only.  `mem` arguments say whether an array lives
+ * in host memory (GPUGRAV_MEM_HOST, copied through pinned staging buffers) or
+ * in device memory of the context's GPU (GPUGRAV_MEM_DEVICE).
+ */
+#ifndef GPUGRAV_H
+#define GPUGRAV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPUGRAV_ABI_VERSION 1
+#define GPUGRAV_MAX_SOFTTYPES 16 /* NSOFTTYPES + NSOFTTYPES_HYDRO supported by this build */
+#define GPUGRAV_NTAB 127         /* NTAB, src/gravity/forcetree.h:86 */
+
+typedef enum gpugrav_status
+{
+  GPUGRAV_OK              = 0,
+  GPUGRAV_ERR_TREE_FULL   = -1,  /* force_treebuild_construct: -1, node storage too small */
+  GPUGRAV_ERR_TOPNODES    = -2,  /* force_treebuild_construct: -2, top-level nodes invalid / do not fit */
+  GPUGRAV_ERR_OUT_OF_BOX  = -3,  /* force_treebuild_construct: -3, particle outside the domain box:
+                                    the caller must redo the domain decomposition (src/gravity/forcetree.c:197-208) */
+  GPUGRAV_ERR_INVALID     = -10, /* bad argument */
+  GPUGRAV_ERR_OOM         = -11, /* device or pinned host allocation failed */
+  GPUGRAV_ERR_CUDA        = -12, /* CUDA runtime error; gpugrav_last_error() has the text */
+  GPUGRAV_ERR_TIMEOUT     = -13, /* a bounded device-side wait gave up (serving loop) */
+  GPUGRAV_ERR_STATE       = -14, /* call order violated (e.g. walk before build) */
+  GPUGRAV_ERR_DEEP_TREE   = -15, /* tree deeper than the walk's fixed limits (pathological input) */
+  GPUGRAV_ERR_UNSUPPORTED = -16  /* option not available in this build */
+} gpugrav_status;
+
+enum
+{
+  GPUGRAV_MEM_HOST   = 0,
+  GPUGRAV_MEM_DEVICE = 1
+};
+
+enum
+{
+  GPUGRAV_PREC_FP64 = 0, /* parity walk: reference arithmetic, per-target opening decisions */
+  GPUGRAV_PREC_FP32 = 1  /* fast walk: FP32 arithmetic, FP64 separations, compensated sums */
+};
+
+/* Run parameters: the All.* fields the path reads. */
+typedef struct gpugrav_params
+{
+  int32_t abi_version;                 /* GPUGRAV_ABI_VERSION */
+  int32_t periodic;                    /* 1: periodic box, TreePM short-range force (PMGRID builds);
+                                          0: isolated, plain Newtonian tree (GRAVITY_NOT_PERIODIC, no PMGRID) */
+  double box_size;                     /* All.BoxSize */
+  double asmth;                        /* All.Asmth[0] (periodic only) */
+  double rcut;                         /* All.Rcut[0] = RCUT * Asmth[0] (periodic only) */
+  double rcut_cells;                   /* RCUT: extent of the tabulated short-range factor (default 4.5) */
+  int32_t nsofttypes;                  /* number of softening types (NSOFTTYPES + NSOFTTYPES_HYDRO) */
+  int32_t type_of_opening_criterion;   /* All.TypeOfOpeningCriterion (0: Barnes-Hut, 1: relative) */
+  double force_softening[GPUGRAV_MAX_SOFTTYPES + 1]; /* All.ForceSoftening[0..nsofttypes], last entry 0
+                                                        (set_softenings, src/gravity/grav_softening.c:92-95) */
+  double err_tol_theta;                /* All.ErrTolTheta; > 0 selects the Barnes-Hut criterion in gpugrav_walk */
+  double err_tol_force_acc;            /* All.ErrTolForceAcc */
+  double top_node_factor;              /* All.TopNodeFactor (library-built top tree only) */
+  int32_t multiple_domains;            /* All.MultipleDomains (library-built top tree only) */
+  int32_t precision;                   /* GPUGRAV_PREC_* */
+} gpugrav_params;
+
+/* Domain geometry: the globals set by domain_findExtent (src/domain/domain_box.c:169-196). */
+typedef struct gpugrav_domain
+{
+  double corner[3];   /* DomainCorner */
+  double center[3];   /* DomainCenter */
+  double len;         /* DomainLen */
+  double inverse_len; /* DomainInverseLen */
+  double big_fac;     /* DomainBigFac = DomainLen / 2^52 */
+} gpugrav_domain;
+
+/* One top-level node: struct topnode_data (src/main/allvars.h:769-782), keys split in two 64-bit halves. */
+typedef struct gpugrav_topnode
+{
+  uint64_t start_key_hi, start_key_lo; /* StartKey (126-bit Peano-Hilbert key) */
+  uint64_t size_hi, size_lo;           /* Size */
+  int32_t daughter;                    /* Daughter: index of the first of 8 daughters, -1 for a leaf */
+  int32_t leaf;                        /* Leaf: top-leaf number (leaves only) */
+  uint8_t morton_to_peano[8];          /* MortonToPeanoSubnode */
+} gpugrav_topnode;
+
+/* Summary of the last build (gpugrav_build). Node indices follow the reference:
+ * particles are [0, max_part), the root node is max_part (Tree_MaxPart), top-level
+ * nodes follow it, first_non_top is Tree_FirstNonTopLevelNode. */
+typedef struct gpugrav_tree_info
+{
+  int64_t num_particles;
+  int64_t max_part;      /* = num_particles */
+  int64_t num_nodes;     /* Tree_NumNodes */
+  int64_t first_non_top; /* Tree_FirstNonTopLevelNode */
+  int32_t num_topnodes;  /* NTopnodes */
+  int32_t num_topleaves; /* NTopleaves */
+  int32_t max_depth;     /* deepest node level (root = 0) */
+  int32_t coincident_cells; /* cells at MAX_TREE_LEVEL holding >= 2 particles */
+} gpugrav_tree_info;
+
+/* Device-time breakdown of the last calls, milliseconds (CUDA events on the library stream). */
+typedef struct gpugrav_timings
+{
+  double upload_ms, domain_ms, sort_ms, toptree_ms, build_ms, moments_ms, walk_ms, download_ms;
+  int64_t interactions; /* sum of per-target interaction counts of the last walk */
+  int32_t walk_kernel_launches;
+  int32_t build_kernel_launches;
+} gpugrav_timings;
+
+typedef struct gpugrav_ctx gpugrav_ctx;
+
+/* ---- lifetime ---- */
+const char *gpugrav_status_string(int32_t status);
+const char *gpugrav_last_error(gpugrav_ctx *ctx);
+int32_t gpugrav_abi_version(void);
+/* Create a context on CUDA device `device`; replaces force_treeallocate (src/gravity/forcetree.c:1677-1696):
+ * the context owns all device memory and grows it as needed. */
+int32_t gpugrav_create(gpugrav_ctx **ctx, int32_t device, const gpugrav_params *params);
+int32_t gpugrav_destroy(gpugrav_ctx *ctx);
+int32_t gpugrav_set_params(gpugrav_ctx *ctx, const gpugrav_params *params);
+/* Run all library work on a caller-owned cudaStream_t (NULL: the context's own stream). */
+int32_t gpugrav_set_stream(gpugrav_ctx *ctx, void *cuda_stream);
+int32_t gpugrav_synchronize(gpugrav_ctx *ctx);
+
+/* ---- domain stage ----
+ * Replaces do_box_wrapping (periodic wrap, src/domain/domain_box.c:259-275), domain_findExtent
+ * (src/domain/domain_box.c:107-197, with DO_NOT_RANDOMIZE_DOMAINCENTER), the key computation of
+ * domain_determineTopTree (src/domain/domain_toplevel.c:120-126) and peano_hilbert_order
+ * (src/domain/peano.c:74-133, a stable sort by key).
+ * pos: n*3 doubles (x,y,z per particle), mass: n doubles, softtype: n bytes (P[].SofteningType).
+ * dom: NULL -> the library computes the extent; otherwise the caller's DomainCorner/Len are used and
+ * a particle outside them yields GPUGRAV_ERR_OUT_OF_BOX (isolated runs, src/gravity/forcetree.c:411-430). */
+int32_t gpugrav_load(gpugrav_ctx *ctx, int64_t n, const double *pos, const double *mass, const uint8_t *softtype,
+                     int32_t mem, const gpugrav_domain *dom);
+
+/* ---- build ----
+ * Replaces force_treebuild (src/gravity/forcetree.c:162-288): top-level skeleton
+ * (force_create_empty_nodes :1131-1180), octree over the 52-bit integer coordinates
+ * (force_treebuild_insert_single_point :835-938, including the MAX_TREE_LEVEL rule for
+ * coincident points), multipole moments and the nextnode/sibling threading
+ * (force_update_node_recursive :1217-1429).
+ * top: the caller's TopNodes (domain_determineTopTree output) or NULL, in which case the library
+ * derives the top tree from the sorted keys with the same refinement rule (one rank, work load =
+ * particle count). */
+int32_t gpugrav_build(gpugrav_ctx *ctx, const gpugrav_topnode *top, int32_t ntop);
+
+/* ---- walk ----
+ * Replaces gravity_tree (src/gravity/gravtree.c:357-707) / force_treeevaluate
+ * (src/gravity/forcetree_walk.c:115-514) for every loaded particle as a target.
+ * The opening criterion follows err_tol_theta: > 0 Barnes-Hut, == 0 relative (uses oldacc).
+ * oldacc: n floats in caller order or NULL (zeros); acc: n*3 doubles; pot, ninter: n each or NULL.
+ * All arrays in caller order, in memory of kind `mem`. */
+int32_t gpugrav_walk(gpugrav_ctx *ctx, const float *oldacc, double *acc, double *pot, int32_t *ninter, int32_t mem);
+
+/* ---- one call: load + build + walk (the drop-in for construct_forcetree + gravity_tree) ---- */
+int32_t gpugrav_compute(gpugrav_ctx *ctx, int64_t n, const double *pos, const double *mass, const uint8_t *softtype,
+                        const float *oldacc, const gpugrav_domain *dom, const gpugrav_topnode *top, int32_t ntop,
+                        double *acc, double *pot, int32_t *ninter, int32_t mem);
+
+/* ---- introspection (parity checks; host buffers) ---- */
+int32_t gpugrav_get_domain(gpugrav_ctx *ctx, gpugrav_domain *dom);
+/* order[i] = caller index of the particle at sorted position i (P[i].ID-1 after peano_hilbert_order) */
+int32_t gpugrav_get_order(gpugrav_ctx *ctx, int64_t *order);
+/* 126-bit keys in sorted order */
+int32_t gpugrav_get_keys(gpugrav_ctx *ctx, uint64_t *key_hi, uint64_t *key_lo);
+int32_t gpugrav_get_topnodes(gpugrav_ctx *ctx, gpugrav_topnode *top, int32_t capacity, int32_t *ntop);
+int32_t gpugrav_get_tree_info(gpugrav_ctx *ctx, gpugrav_tree_info *info);
+/* Nodes in the reference's numbering: entry k describes node max_part + k, k < num_nodes.
+ * center, s: 3 doubles per node; p_next, p_father: per particle (sorted order). Any pointer may be NULL. */
+int32_t gpugrav_export_tree(gpugrav_ctx *ctx, double *center, double *len, double *s, double *mass, int32_t *sibling,
+                            int32_t *nextnode, int32_t *father, uint8_t *maxsofttype, int32_t *p_next, int32_t *p_father);
+int32_t gpugrav_get_timings(gpugrav_ctx *ctx, gpugrav_timings *t);
+
+/* ---- direct summation (accuracy instrument; gravity_forcetest_evaluate,
+ *      src/gravity/gravtree_forcetest.c:421-648, without Ewald images) ----
+ * FP64 direct sum over all loaded particles for the given targets (caller indices):
+ * the TreePM short-range force with the exact erfc factor (periodic) or Newtonian (isolated). */
+int32_t gpugrav_direct(gpugrav_ctx *ctx, int64_t ntargets, const int64_t *targets, double *acc, double *pot);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPUGRAV_H */
