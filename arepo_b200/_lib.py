@@ -36,6 +36,8 @@ MEM_HOST = 0
 MEM_DEVICE = 1
 PREC_FP64 = 0
 PREC_FP32 = 1
+DIRECT_FULL = 0
+DIRECT_CUT = 1
 
 
 class Params(C.Structure):
@@ -130,7 +132,8 @@ _SIGS = {
     "gpugrav_get_tree_info": (C.c_int32, [_P, C.POINTER(TreeInfo)]),
     "gpugrav_export_tree": (C.c_int32, [_P] + [_P] * 10),
     "gpugrav_get_timings": (C.c_int32, [_P, C.POINTER(Timings)]),
-    "gpugrav_direct": (C.c_int32, [_P, C.c_int64, _P, _P, _P]),
+    "gpugrav_direct": (C.c_int32, [_P, C.c_int64, _P, C.c_int32, _P, _P]),
+    "gpugrav_measure_fma_peak": (C.c_int32, [C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
 }
 
 _lib = None

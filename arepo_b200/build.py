@@ -27,6 +27,7 @@ SOURCES = [
     ("walk64.cu", True),
     ("direct.cu", True),
     ("walk32.cu", False),
+    ("peak.cu", False),
     ("gpugrav.cu", True),
 ]
 

@@ -34,7 +34,7 @@ constexpr int kChunks = 64;   // source chunks
 
 __global__ void __launch_bounds__(kTile) k_direct(const double4 *__restrict__ pm, const uint8_t *__restrict__ st, int64_t n,
                                                   const int64_t *__restrict__ targets_sorted, int64_t nt,
-                                                  const WalkConst *__restrict__ wcp, double4 *__restrict__ partial)
+                                                  const WalkConst *__restrict__ wcp, int cut, double4 *__restrict__ partial)
 {
   __shared__ double4 src[kTile];
   __shared__ double hsrc[kTile];
@@ -76,6 +76,8 @@ __global__ void __launch_bounds__(kTile) k_direct(const double4 *__restrict__ pm
                 dz = (dz > w.half_box) ? dz - w.box : ((dz < -w.half_box) ? dz + w.box : dz);
               }
             double r2 = dx * dx + dy * dy + dz * dz;
+            if(cut && w.periodic && !(r2 < w.rcut2))
+              continue;  // beyond Rcut: the part of the force left to the PM mesh
             double r  = sqrt(r2);
             double m  = s.w;
             double h_j  = hsrc[q];
@@ -160,7 +162,8 @@ __global__ void k_map_targets(const int64_t *__restrict__ tg, int64_t nt, const 
 }
 }  // namespace
 
-cudaError_t direct_stage(gpugrav_ctx *c, const WalkConst &wc, int64_t nt, const int64_t *d_targets, double *d_acc, double *d_pot)
+cudaError_t direct_stage(gpugrav_ctx *c, const WalkConst &wc, int64_t nt, const int64_t *d_targets, int cut, double *d_acc,
+                         double *d_pot)
 {
   (void)wc;
   if(nt == 0)
@@ -175,7 +178,7 @@ cudaError_t direct_stage(gpugrav_ctx *c, const WalkConst &wc, int64_t nt, const 
   k_map_targets<<<(unsigned)((nt + 255) / 256), 256, 0, c->stream>>>(d_targets, nt, inv.as<int32_t>(), ts.as<int64_t>());
   dim3 grid((unsigned)((nt + kTile - 1) / kTile), kChunks);
   k_direct<<<grid, kTile, 0, c->stream>>>(c->s_pm.as<double4>(), c->s_st.as<uint8_t>(), c->n, ts.as<int64_t>(), nt,
-                                         c->wconst.as<WalkConst>(), part.as<double4>());
+                                         c->wconst.as<WalkConst>(), cut, part.as<double4>());
   k_direct_reduce<<<(unsigned)((nt + 255) / 256), 256, 0, c->stream>>>(part.as<double4>(), nt, d_acc, d_pot);
   e = cudaGetLastError();
   cudaStreamSynchronize(c->stream);

@@ -701,9 +701,9 @@ int32_t gpugrav_get_timings(gpugrav_ctx *c, gpugrav_timings *t)
   return GPUGRAV_OK;
 }
 
-int32_t gpugrav_direct(gpugrav_ctx *c, int64_t ntargets, const int64_t *targets, double *acc, double *pot)
+int32_t gpugrav_direct(gpugrav_ctx *c, int64_t ntargets, const int64_t *targets, int32_t mode, double *acc, double *pot)
 {
-  if(!c || ntargets < 0 || (ntargets > 0 && (!targets || !acc)))
+  if(!c || ntargets < 0 || (ntargets > 0 && (!targets || !acc)) || (mode != GPUGRAV_DIRECT_FULL && mode != GPUGRAV_DIRECT_CUT))
     return GPUGRAV_ERR_INVALID;
   if(!c->loaded)
     return fail(c, GPUGRAV_ERR_STATE, "gpugrav_direct before gpugrav_load");
@@ -720,7 +720,8 @@ int32_t gpugrav_direct(gpugrav_ctx *c, int64_t ntargets, const int64_t *targets,
   make_walk_const(c->prm, &wc);
   CK(cudaMemcpyAsync(c->wconst.p, &wc, sizeof(wc), cudaMemcpyHostToDevice, st), "walk constants");
   CK(cudaMemcpyAsync(dt.p, targets, ntargets * 8, cudaMemcpyHostToDevice, st), "targets");
-  CK(gg::direct_stage(c, wc, ntargets, dt.as<int64_t>(), da.as<double>(), dp.as<double>()), "direct summation");
+  CK(gg::direct_stage(c, wc, ntargets, dt.as<int64_t>(), mode == GPUGRAV_DIRECT_CUT, da.as<double>(), dp.as<double>()),
+     "direct summation");
   CK(cudaMemcpyAsync(acc, da.p, ntargets * 24, cudaMemcpyDeviceToHost, st), "download");
   if(pot)
     CK(cudaMemcpyAsync(pot, dp.p, ntargets * 8, cudaMemcpyDeviceToHost, st), "download");

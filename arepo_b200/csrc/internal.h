@@ -132,7 +132,7 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status);
 cudaError_t walk64_stage(gpugrav_ctx *c, const WalkConst &wc);
 cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc);
 cudaError_t layout32_stage(gpugrav_ctx *c);
-cudaError_t direct_stage(gpugrav_ctx *c, const WalkConst &wc, int64_t nt, const int64_t *d_targets, double *d_acc,
+cudaError_t direct_stage(gpugrav_ctx *c, const WalkConst &wc, int64_t nt, const int64_t *d_targets, int cut, double *d_acc,
                          double *d_pot);
 void make_walk_const(const gpugrav_params &p, WalkConst *wc);
 }  // namespace gg

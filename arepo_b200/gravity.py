@@ -176,10 +176,12 @@ class GravityTree:
         self._check(self.lib.gpugrav_get_timings(self._ctx, C.byref(t)))
         return t
 
-    def direct(self, targets) -> tuple[np.ndarray, np.ndarray]:
-        """FP64 direct summation for the given caller indices (accuracy instrument)."""
+    def direct(self, targets, cut: bool = False) -> tuple[np.ndarray, np.ndarray]:
+        """FP64 direct summation for the given caller indices (accuracy instrument). cut=True keeps
+        only pairs closer than Rcut (the range the walk evaluates) in a periodic TreePM run."""
         tg = np.ascontiguousarray(targets, np.int64)
         acc = np.empty((len(tg), 3))
         pot = np.empty(len(tg))
-        self._check(self.lib.gpugrav_direct(self._ctx, len(tg), L.ptr(tg), L.ptr(acc), L.ptr(pot)))
+        self._check(self.lib.gpugrav_direct(self._ctx, len(tg), L.ptr(tg), L.DIRECT_CUT if cut else L.DIRECT_FULL,
+                                                    L.ptr(acc), L.ptr(pot)))
         return acc, pot

@@ -197,8 +197,21 @@ int32_t gpugrav_get_timings(gpugrav_ctx *ctx, gpugrav_timings *t);
 /* ---- direct summation (accuracy instrument; gravity_forcetest_evaluate,
  *      src/gravity/gravtree_forcetest.c:421-648, without Ewald images) ----
  * FP64 direct sum over all loaded particles for the given targets (caller indices):
- * the TreePM short-range force with the exact erfc factor (periodic) or Newtonian (isolated). */
-int32_t gpugrav_direct(gpugrav_ctx *ctx, int64_t ntargets, const int64_t *targets, double *acc, double *pot);
+ * the TreePM short-range force with the exact erfc factor (periodic) or Newtonian (isolated).
+ * mode GPUGRAV_DIRECT_FULL sums every pair (gravtree_forcetest.c:583-601); GPUGRAV_DIRECT_CUT keeps
+ * only pairs closer than Rcut, the range the tree walk evaluates (forcetree_walk.c:369-372), so that
+ * the difference to the walk is the tree approximation error alone. */
+enum
+{
+  GPUGRAV_DIRECT_FULL = 0,
+  GPUGRAV_DIRECT_CUT  = 1
+};
+int32_t gpugrav_direct(gpugrav_ctx *ctx, int64_t ntargets, const int64_t *targets, int32_t mode, double *acc, double *pot);
+
+/* ---- diagnostics (no counterpart in the reference) ----
+ * CUDA-core fused multiply-add throughput of `device` in TFLOP/s for GPUGRAV_PREC_FP32 or
+ * GPUGRAV_PREC_FP64 (2 flops per FMA): the denominator of the tree walk's roofline. */
+int32_t gpugrav_measure_fma_peak(int32_t device, int32_t precision, double *tflops);
 
 #ifdef __cplusplus
 }
