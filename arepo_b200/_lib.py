@@ -31,6 +31,7 @@ ERR_TIMEOUT = -13
 ERR_STATE = -14
 ERR_DEEP_TREE = -15
 ERR_UNSUPPORTED = -16
+ERR_TOO_LARGE = -17
 
 MEM_HOST = 0
 MEM_DEVICE = 1
@@ -133,6 +134,8 @@ _SIGS = {
     "gpugrav_export_tree": (C.c_int32, [_P] + [_P] * 10),
     "gpugrav_get_timings": (C.c_int32, [_P, C.POINTER(Timings)]),
     "gpugrav_direct": (C.c_int32, [_P, C.c_int64, _P, C.c_int32, _P, _P]),
+    "gpugrav_direct_noalloc": (C.c_int32, [C.c_int32, C.POINTER(Params), C.c_int64, _P, _P, _P, C.c_int64, _P, _P,
+                                            C.c_int32, _P, _P, _P]),
     "gpugrav_measure_fma_peak": (C.c_int32, [C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
 }
 

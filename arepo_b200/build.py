@@ -26,6 +26,7 @@ SOURCES = [
     ("tree.cu", True),
     ("walk64.cu", True),
     ("direct.cu", True),
+    ("direct_noalloc.cu", True),
     ("walk32.cu", False),
     ("peak.cu", False),
     ("gpugrav.cu", True),

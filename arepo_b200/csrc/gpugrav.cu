@@ -246,6 +246,8 @@ const char *gpugrav_status_string(int32_t s)
         return "tree deeper than supported";
       case GPUGRAV_ERR_UNSUPPORTED:
         return "unsupported option";
+      case GPUGRAV_ERR_TOO_LARGE:
+        return "request exceeds a fixed capacity (gpugrav_direct_noalloc: at most 4096 targets per call)";
       default:
         return "unknown status";
     }

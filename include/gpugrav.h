@@ -50,7 +50,8 @@ typedef enum gpugrav_status
   GPUGRAV_ERR_TIMEOUT     = -13, /* a bounded device-side wait gave up (serving loop) */
   GPUGRAV_ERR_STATE       = -14, /* call order violated (e.g. walk before build) */
   GPUGRAV_ERR_DEEP_TREE   = -15, /* tree deeper than the walk's fixed limits (pathological input) */
-  GPUGRAV_ERR_UNSUPPORTED = -16  /* option not available in this build */
+  GPUGRAV_ERR_UNSUPPORTED = -16, /* option not available in this build */
+  GPUGRAV_ERR_TOO_LARGE   = -17  /* request exceeds a fixed capacity (gpugrav_direct_noalloc: 4096 targets) */
 } gpugrav_status;
 
 enum
@@ -207,6 +208,21 @@ enum
   GPUGRAV_DIRECT_CUT  = 1
 };
 int32_t gpugrav_direct(gpugrav_ctx *ctx, int64_t ntargets, const int64_t *targets, int32_t mode, double *acc, double *pot);
+
+/* ---- direct summation without allocation (no counterpart in the reference) ----
+ * The same FP64 sum as gpugrav_direct, for callers that cannot allocate device memory at the point
+ * of the call (their device memory belongs to their own pool allocator, or they cannot accept the
+ * device-wide synchronisation of cudaMalloc/cudaFree mid-step). Needs no context: every array is the
+ * caller's, in device memory of `device` -- pos (n*3), mass (n), softtype (n) of the sources, inside
+ * the periodic box for periodic runs; target_pos (ntargets*3), target_softtype (ntargets); outputs
+ * acc (ntargets*3) and pot (ntargets or NULL). Launches on `stream` (a cudaStream_t, NULL = default)
+ * and returns without synchronising. At most 4096 targets per call (GPUGRAV_ERR_TOO_LARGE beyond);
+ * its scratch is a fixed 4 MiB device array per GPU, held until exit and shared by all calls: calls
+ * that overlap on the GPU race. The first call on a device resolves the array's address; make it
+ * before any stream capture. Allocates nothing (no cudaMalloc/cudaFree). */
+int32_t gpugrav_direct_noalloc(int32_t device, const gpugrav_params *params, int64_t n, const double *pos,
+                               const double *mass, const uint8_t *softtype, int64_t ntargets, const double *target_pos,
+                               const uint8_t *target_softtype, int32_t mode, double *acc, double *pot, void *stream);
 
 /* ---- diagnostics (no counterpart in the reference) ----
  * CUDA-core fused multiply-add throughput of `device` in TFLOP/s for GPUGRAV_PREC_FP32 or
