@@ -308,7 +308,7 @@ int32_t gpugrav_destroy(gpugrav_ctx *c)
                         &c->cnt, &c->base, &c->hcnt, &c->hack_list, &c->hack_scratch, &c->counters, &c->top, &c->skel,
                         &c->n_suns, &c->n_depth, &c->n_cl, &c->n_sm, &c->n_maxsoft, &c->n_size, &c->n_father, &c->n_sibling,
                         &c->n_next, &c->n_dfs, &c->n_first, &c->p_next, &c->p_father, &c->p_dfs, &c->depth_hist,
-                        &c->depth_order, &c->w_sm, &c->w_cl, &c->w_link, &c->w32_a, &c->w32_b, &c->acc_s, &c->pot_s,
+                        &c->depth_order, &c->w_sm, &c->w_cl, &c->w_link, &c->g_key, &c->g_key_alt, &c->g_val, &c->g_val_alt, &c->g_bfs, &c->g_np, &c->g_poff, &c->g_sm, &c->g_rel, &c->g_kids, &c->g_pm, &c->g_pst, &c->g_stack, &c->acc_s, &c->pot_s,
                         &c->nint_s, &c->oldacc_s, &c->oldacc_in, &c->out_acc, &c->out_pot, &c->out_nint, &c->scratch};
   for(auto *b : bufs)
     b->release();
@@ -443,6 +443,7 @@ int32_t gpugrav_build(gpugrav_ctx *c, const gpugrav_topnode *top, int32_t ntop)
   DeviceGuard g(c->device);
   cudaStream_t st = c->stream;
   c->built        = false;
+  c->layout32_valid = false;
   cudaEventRecord(c->ev[4], st);
   if(top)
     {
@@ -507,6 +508,7 @@ int32_t gpugrav_walk(gpugrav_ctx *c, const float *oldacc, double *acc, double *p
     }
   k_gather_f32<<<grid_for(n, 256), 256, 0, st>>>(old_dev, c->perm.as<uint32_t>(), n, c->oldacc_s.as<float>());
   CK(cudaMemsetAsync(c->counters.as<int>() + 32, 0, 8, st), "reset counters");
+  CK(cudaMemsetAsync(c->counters.as<int>() + 14, 0, 4, st), "reset counters");
   cudaEventRecord(c->ev[8], st);
   if(c->prm.precision == GPUGRAV_PREC_FP32)
     {
@@ -540,9 +542,13 @@ int32_t gpugrav_walk(gpugrav_ctx *c, const float *oldacc, double *acc, double *p
         CK(cudaMemcpyAsync(ninter, d_nint, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "download interactions");
     }
   unsigned long long tot = 0;
+  int walk_err = 0;
   CK(cudaMemcpyAsync(&tot, c->counters.as<int>() + 32, 8, cudaMemcpyDeviceToHost, st), "interaction total");
+  CK(cudaMemcpyAsync(&walk_err, c->counters.as<int>() + 14, 4, cudaMemcpyDeviceToHost, st), "walk flags");
   cudaEventRecord(c->ev[10], st);
   CK(cudaStreamSynchronize(st), "walk");
+  if(walk_err)
+    return fail(c, GPUGRAV_ERR_DEEP_TREE, "gpugrav_walk: traversal stack of the FP32 walk exhausted");
   c->timings.walk_ms              = elapsed(c->ev[8], c->ev[9]);
   c->timings.download_ms          = elapsed(c->ev[9], c->ev[10]);
   c->timings.interactions         = (int64_t)tot;

@@ -110,7 +110,13 @@ struct gpugrav_ctx
   gg::DevBuf p_next, p_father, p_dfs;
   gg::DevBuf depth_hist, depth_order;
   gg::DevBuf w_sm, w_cl, w_link;              // walk layout (DFS order)
-  gg::DevBuf w32_a, w32_b;                    // FP32 walk layout
+  // FP32 group walk: nodes in breadth-first order (children contiguous), particles grouped by parent
+  gg::DevBuf g_key, g_key_alt, g_val, g_val_alt, g_bfs;   // (depth, dfs) sort -> breadth-first rank
+  gg::DevBuf g_np, g_poff;                    // particle children per node (bfs order), their offsets
+  gg::DevBuf g_sm, g_rel, g_kids;             // node: (CoM, mass) double4; (centre - CoM, len) float4; int4 links
+  gg::DevBuf g_pm, g_pst;                     // particles in parent order: (x, y, z, m) double4; softening type
+  gg::DevBuf g_stack;                         // per-warp traversal stacks
+  bool layout32_valid = false;
   gg::DevBuf acc_s, pot_s, nint_s, oldacc_s, oldacc_in;  // per target (sorted), inputs
   gg::DevBuf out_acc, out_pot, out_nint;      // caller order staging for host copies
   gg::DevBuf scratch;                         // reductions

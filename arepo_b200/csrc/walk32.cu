@@ -1,17 +1,575 @@
-// walk32.cu -- FP32 walk (placeholder until the fast kernel lands): refuses.
+// walk32.cu -- FP32 group walk (the fast path).
+//
+// Physics as in force_treeevaluate (src/gravity/forcetree_walk.c:115-514): the
+// tabulated erfc short-range factor cut at Rcut, the cubic-spline softening, the
+// periodic nearest image, the relative criterion (ErrTolForceAcc x OldAcc) after
+// a Barnes-Hut pass.  Different arithmetic organisation:
+//
+//  * a warp walks the tree for a group of 32 targets that are consecutive in key
+//    order (compact in space); nodes are tested 32 at a time, one per lane,
+//    against the group's bounding box with the reference's tests made
+//    conservative for the whole group (a node is accepted only if every target of
+//    the group would accept it), so each target's error is at most that of its
+//    own reference walk;
+//  * accepted nodes and the particles of opened nodes go to an interaction list
+//    in shared memory; the list is evaluated densely -- every lane computes its
+//    own target against every entry -- in FP32;
+//  * separations: the group centre g is subtracted in FP64 from every list
+//    entry and from every target before rounding to FP32, so an FP32 difference
+//    never carries the absolute position (error ~ eps32 x |x - g|, not eps32 x |x|);
+//  * sums: FP32 within a list batch, batch partials accumulated in FP64.
+//
+// Layout: nodes in breadth-first order with contiguous children (ranked by
+// (depth, depth-first position)), particles grouped by parent node.
+#include <cub/cub.cuh>
+
 #include "internal.h"
 
 namespace gg
 {
-cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc)
+namespace
 {
-  (void)c;
-  (void)wc;
-  return cudaErrorNotSupported;
+constexpr int kWarps    = 4;      // warps per block
+constexpr int kListCap  = 448;    // interaction list entries per warp
+constexpr int kEvalAt   = 160;    // evaluate once this many entries are queued
+constexpr int kStackCap = 16384;  // traversal stack entries per warp (global memory)
+
+#define SF1 10.666666666667f
+#define SF2 32.0f
+#define SF3 (-38.4f)
+#define SF4 (-2.8f)
+#define SF5 5.333333333333f
+#define SF6 6.4f
+#define SF7 (-9.6f)
+#define SF8 21.333333333333f
+#define SF9 (-48.0f)
+#define SF10 38.4f
+#define SF11 (-10.666666666667f)
+#define SF12 (-0.066666666667f)
+#define SF13 (-3.2f)
+#define SF14 0.066666666667f
+#define SF15 (-16.0f)
+#define SF16 9.6f
+#define SF17 (-2.133333333333f)
+
+struct W32Const
+{
+  double box, half_box;
+  float rcut, rcut2, asmthfac, asmthinv2;
+  float theta2, erracc;
+  int periodic, bh;
+  float soft[GPUGRAV_MAX_SOFTTYPES + 1];
+  float2 tab[kNtab + 1];   // (f[i], f[i+1] - f[i]) of the force table
+  float2 tabp[kNtab + 1];  // same for the potential table
+};
+
+// ------------------------------------------------------------------------------
+// layout
+// ------------------------------------------------------------------------------
+__global__ void k_g_keys(int64_t nn, const uint8_t *__restrict__ depth, const int32_t *__restrict__ ndfs,
+                         uint64_t *__restrict__ key, int32_t *__restrict__ val)
+{
+  for(int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nn; k += (int64_t)gridDim.x * blockDim.x)
+    {
+      key[k] = ((uint64_t)depth[k] << 32) | (uint32_t)ndfs[k];
+      val[k] = (int32_t)k;
+    }
 }
+
+__global__ void k_g_rank(int64_t nn, int64_t n, const int32_t *__restrict__ sorted, const int32_t *__restrict__ suns,
+                         int32_t *__restrict__ bfs, int32_t *__restrict__ np)
+{
+  for(int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < nn; b += (int64_t)gridDim.x * blockDim.x)
+    {
+      int32_t k = sorted[b];
+      bfs[k]    = (int32_t)b;
+      int c     = 0;
+      for(int q = 0; q < 8; q++)
+        {
+          int32_t v = suns[8 * (int64_t)k + q];
+          c += (v >= 0 && v < n) ? 1 : 0;
+        }
+      np[b] = c;
+    }
+}
+
+__global__ void k_g_fill(int64_t nn, int64_t n, const int32_t *__restrict__ sorted, const int32_t *__restrict__ suns,
+                         const int32_t *__restrict__ bfs, const int32_t *__restrict__ poff, const double4 *__restrict__ sm,
+                         const double4 *__restrict__ cl, const uint8_t *__restrict__ maxsoft, const double4 *__restrict__ pm,
+                         const uint8_t *__restrict__ st, double4 *__restrict__ g_sm, float4 *__restrict__ g_rel,
+                         int4 *__restrict__ g_kids, double4 *__restrict__ g_pm, uint8_t *__restrict__ g_pst, int *err)
+{
+  for(int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < nn; b += (int64_t)gridDim.x * blockDim.x)
+    {
+      int32_t k = sorted[b];
+      double4 s = sm[k], c = cl[k];
+      g_sm[b]   = s;
+      g_rel[b]  = make_float4((float)(c.x - s.x), (float)(c.y - s.y), (float)(c.z - s.z), (float)c.w);
+      int32_t fc = -1, nc = 0, npc = 0;
+      int32_t fp = poff[b];
+      for(int q = 0; q < 8; q++)
+        {
+          int32_t v = suns[8 * (int64_t)k + q];
+          if(v < 0)
+            continue;
+          if(v < n)
+            {
+              g_pm[fp + npc]  = pm[v];
+              g_pst[fp + npc] = st[v];
+              npc++;
+            }
+          else
+            {
+              int32_t cb = bfs[v - n];
+              if(fc < 0)
+                fc = cb;
+              else if(cb != fc + nc)
+                atomicOr(err, 8);  // children must be contiguous in breadth-first order
+              nc++;
+            }
+        }
+      g_kids[b] = make_int4(fc, fp, nc | (npc << 4), (int)maxsoft[k]);
+    }
+}
+
+// ------------------------------------------------------------------------------
+// walk
+// ------------------------------------------------------------------------------
+__device__ __forceinline__ double wrapd(double d, const W32Const &w)
+{
+  if(!w.periodic)
+    return d;
+  return (d > w.half_box) ? d - w.box : ((d < -w.half_box) ? d + w.box : d);
+}
+
+__device__ __forceinline__ double wmin(double v)
+{
+  for(int o = 16; o > 0; o >>= 1)
+    v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double wmax(double v)
+{
+  for(int o = 16; o > 0; o >>= 1)
+    v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ float wminf(float v)
+{
+  for(int o = 16; o > 0; o >>= 1)
+    v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ int wscan_incl(int v, int lane)
+{
+  for(int o = 1; o < 32; o <<= 1)
+    {
+      int u = __shfl_up_sync(0xffffffffu, v, o);
+      if(lane >= o)
+        v += u;
+    }
+  return v;
+}
+
+template <bool POT>
+__device__ __forceinline__ void evaluate(const float4 *__restrict__ LP, const float *__restrict__ LH, int nl, float xr, float yr,
+                                         float zr, float hi, const W32Const &w, float &ax, float &ay, float &az, float &pot,
+                                         int &ni)
+{
+#pragma unroll 4
+  for(int j = 0; j < nl; j++)
+    {
+      const float4 e = LP[j];
+      const float hj = LH[j];
+      const float dx = e.x - xr, dy = e.y - yr, dz = e.z - zr;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      if(w.periodic && !(r2 < w.rcut2))
+        continue;
+      const float hmax = fmaxf(hi, hj);
+      const float rinv = (r2 > 0.0f) ? rsqrtf(r2) : 0.0f;
+      const float r    = r2 * rinv;
+      float ff = 0.0f, fpt = 0.0f;
+      if(w.periodic)
+        {
+          const float te = r * w.asmthfac;
+          int ti         = (int)te;
+          ti             = ti < kNtab - 1 ? ti : kNtab - 1;
+          const float tw = te - (float)ti;
+          const float2 tb = w.tab[ti];
+          ff             = fmaf(tw, tb.y, tb.x);
+          if(POT)
+            {
+              const float2 tp = w.tabp[ti];
+              fpt             = fmaf(tw, tp.y, tp.x);
+            }
+        }
+      float fac, wp = 0.0f;
+      if(r >= hmax)
+        {
+          const float rinv2 = rinv * rinv;
+          fac               = rinv2 * rinv;
+          if(w.periodic)
+            {
+              fac = fmaf(rinv * ff, w.asmthinv2, fac);
+              if(POT)
+                wp = rinv * fpt;
+            }
+          else if(POT)
+            wp = -rinv;
+        }
+      else
+        {
+          const float h_inv  = 1.0f / hmax;
+          const float h3_inv = h_inv * h_inv * h_inv;
+          const float u      = r * h_inv;
+          const float u2     = u * u;
+          if(u < 0.5f)
+            {
+              fac = h3_inv * fmaf(u2, fmaf(SF2, u, SF3), SF1);
+              if(POT)
+                wp = h_inv * fmaf(u2, fmaf(u2, fmaf(SF6, u, SF7), SF5), SF4);
+            }
+          else
+            {
+              const float u3 = u2 * u;
+              fac = h3_inv * (SF8 + SF9 * u + SF10 * u2 + SF11 * u3 + SF12 / u3);
+              if(POT)
+                wp = h_inv * (SF13 + SF14 / u + u2 * (SF1 + u * (SF15 + u * (SF16 + SF17 * u))));
+            }
+          if(w.periodic && r > 0.0f)
+            {
+              fac = fmaf(rinv * ff, w.asmthinv2, fac);
+              if(POT)
+                wp = fmaf(rinv, fpt + 1.0f, wp);
+            }
+        }
+      if(e.w != 0.0f)
+        {
+          const float fm = fac * e.w;
+          ax             = fmaf(dx, fm, ax);
+          ay             = fmaf(dy, fm, ay);
+          az             = fmaf(dz, fm, az);
+          if(POT)
+            pot = fmaf(e.w, wp, pot);
+          ni++;
+        }
+    }
+}
+
+template <bool POT>
+__global__ void __launch_bounds__(32 * kWarps) k_walk32(const double4 *__restrict__ g_sm, const float4 *__restrict__ g_rel,
+                                                        const int4 *__restrict__ g_kids, const double4 *__restrict__ g_pm,
+                                                        const uint8_t *__restrict__ g_pst, const double4 *__restrict__ tpm,
+                                                        const uint8_t *__restrict__ tst, const float *__restrict__ oldacc,
+                                                        int64_t n, int ngroups, const W32Const *__restrict__ wcp,
+                                                        int *__restrict__ stack_base, int *__restrict__ work,
+                                                        double *__restrict__ acc_out, double *__restrict__ pot_out,
+                                                        int32_t *__restrict__ nint_out, unsigned long long *__restrict__ total,
+                                                        int *__restrict__ err)
+{
+  __shared__ W32Const w;
+  __shared__ float4 il_p[kWarps][kListCap];
+  __shared__ float il_h[kWarps][kListCap];
+  for(int t = threadIdx.x; t < (int)(sizeof(W32Const) / 4); t += blockDim.x)
+    ((int *)&w)[t] = ((const int *)wcp)[t];
+  __syncthreads();
+
+  const int warp         = threadIdx.x >> 5;
+  const int lane         = threadIdx.x & 31;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  int *stack             = stack_base + ((int64_t)blockIdx.x * kWarps + warp) * kStackCap;
+  float4 *LP             = il_p[warp];
+  float *LH              = il_h[warp];
+  unsigned long long my_total = 0;
+
+  while(true)
+    {
+      int grp = 0;
+      if(lane == 0)
+        grp = atomicAdd(work, 1);
+      grp = __shfl_sync(0xffffffffu, grp, 0);
+      if(grp >= ngroups)
+        break;
+      const int64_t t0   = (int64_t)grp * 32;
+      const int64_t t    = t0 + lane;
+      const bool valid   = t < n;
+      const int64_t tt   = valid ? t : t0;
+      const double4 p    = tpm[tt];
+      // group box (FP64), centre g, half extent
+      const double mnx = wmin(p.x), mxx = wmax(p.x), mny = wmin(p.y), mxy = wmax(p.y), mnz = wmin(p.z), mxz = wmax(p.z);
+      const double gx = 0.5 * (mnx + mxx), gy = 0.5 * (mny + mxy), gz = 0.5 * (mnz + mxz);
+      const float ex = (float)(0.5 * (mxx - mnx)) * 1.000001f, ey = (float)(0.5 * (mxy - mny)) * 1.000001f,
+                  ez = (float)(0.5 * (mxz - mnz)) * 1.000001f;
+      const float xr = (float)(p.x - gx), yr = (float)(p.y - gy), zr = (float)(p.z - gz);
+      const float hi = w.soft[tst[tt]];
+      const float h_min = wminf(hi);
+      const float aold_min = wminf(w.erracc * oldacc[tt]);
+
+      double dax = 0, day = 0, daz = 0, dpot = 0;
+      float ax = 0, ay = 0, az = 0, pt = 0;
+      int ni = 0;
+      int nl = 0, sp = 1;
+      if(lane == 0)
+        stack[0] = 0;  // root
+      __syncwarp();
+
+      while(sp > 0)
+        {
+          const int take = sp < 32 ? sp : 32;
+          sp -= take;
+          int node = -1;
+          if(lane < take)
+            node = stack[sp + lane];
+          __syncwarp();
+
+          int action = 0;  // 1 accept, 2 open
+          float4 entry = make_float4(0, 0, 0, 0);
+          float hj     = 0;
+          int fc = 0, fp = 0, nc = 0, np = 0;
+          if(node >= 0)
+            {
+              const double4 sm = g_sm[node];
+              if(sm.w != 0.0)
+                {
+                  const float4 rel = g_rel[node];
+                  const int4 kd    = g_kids[node];
+                  const float sx = (float)wrapd(sm.x - gx, w), sy = (float)wrapd(sm.y - gy, w), sz = (float)wrapd(sm.z - gz, w);
+                  const float cx = sx + rel.x, cy = sy + rel.y, cz = sz + rel.z;
+                  const float L  = rel.w;
+                  const float m  = (float)sm.w;
+                  hj             = w.soft[kd.w];
+                  bool prune     = false;
+                  if(w.periodic)
+                    {
+                      const float eff = w.rcut + 0.5f * L;
+                      prune = (fabsf(cx) - ex > eff) || (fabsf(cy) - ey > eff) || (fabsf(cz) - ez > eff);
+                    }
+                  if(!prune)
+                    {
+                      const float dmx = fmaxf(fabsf(sx) - ex, 0.0f), dmy = fmaxf(fabsf(sy) - ey, 0.0f),
+                                  dmz = fmaxf(fabsf(sz) - ez, 0.0f);
+                      const float rmin2 = dmx * dmx + dmy * dmy + dmz * dmz;
+                      const float L2    = L * L;
+                      bool open;
+                      if(w.bh)
+                        open = L2 > rmin2 * w.theta2;
+                      else
+                        open = (L2 > rmin2 * 1.44f) || (m * L2 > rmin2 * rmin2 * aold_min) ||
+                               (fabsf(cx) < 0.6f * L + ex && fabsf(cy) < 0.6f * L + ey && fabsf(cz) < 0.6f * L + ez);
+                      if(!open && hj > h_min && rmin2 < hj * hj)
+                        open = true;
+                      if(open)
+                        {
+                          action = 2;
+                          fc     = kd.x;
+                          fp     = kd.y;
+                          nc     = kd.z & 15;
+                          np     = (kd.z >> 4) & 15;
+                        }
+                      else
+                        {
+                          action = 1;
+                          entry  = make_float4(sx, sy, sz, m);
+                        }
+                    }
+                }
+            }
+          // accepted nodes -> list
+          const unsigned am = __ballot_sync(0xffffffffu, action == 1);
+          if(action == 1)
+            {
+              const int pos = nl + __popc(am & lt_mask);
+              LP[pos]       = entry;
+              LH[pos]       = hj;
+            }
+          nl += __popc(am);
+          // particles of opened nodes -> list
+          const int npx  = (action == 2) ? np : 0;
+          const int pinc = wscan_incl(npx, lane);
+          const int ptot = __shfl_sync(0xffffffffu, pinc, 31);
+          {
+            const int pb = nl + pinc - npx;
+            for(int q = 0; q < npx; q++)
+              {
+                const double4 pp = g_pm[fp + q];
+                LP[pb + q] = make_float4((float)wrapd(pp.x - gx, w), (float)wrapd(pp.y - gy, w), (float)wrapd(pp.z - gz, w),
+                                         (float)pp.w);
+                LH[pb + q] = w.soft[g_pst[fp + q]];
+              }
+          }
+          nl += ptot;
+          // node children of opened nodes -> stack (contiguous in breadth-first order)
+          const int ncx  = (action == 2) ? nc : 0;
+          const int cinc = wscan_incl(ncx, lane);
+          const int ctot = __shfl_sync(0xffffffffu, cinc, 31);
+          if(sp + ctot <= kStackCap)
+            {
+              const int cb = sp + cinc - ncx;
+              for(int q = 0; q < ncx; q++)
+                stack[cb + q] = fc + q;
+              sp += ctot;
+            }
+          else if(lane == 0)
+            atomicOr(err, 16);  // stack too small: the walk of this group is incomplete
+          __syncwarp();
+          if(nl >= kEvalAt)
+            {
+              evaluate<POT>(LP, LH, nl, xr, yr, zr, hi, w, ax, ay, az, pt, ni);
+              dax += ax;
+              day += ay;
+              daz += az;
+              dpot += pt;
+              ax = ay = az = pt = 0;
+              nl = 0;
+              __syncwarp();
+            }
+        }
+      if(nl > 0)
+        {
+          evaluate<POT>(LP, LH, nl, xr, yr, zr, hi, w, ax, ay, az, pt, ni);
+          dax += ax;
+          day += ay;
+          daz += az;
+          dpot += pt;
+          __syncwarp();
+        }
+      if(valid)
+        {
+          acc_out[3 * t + 0] = dax;
+          acc_out[3 * t + 1] = day;
+          acc_out[3 * t + 2] = daz;
+          if(POT)
+            pot_out[t] = dpot;
+          nint_out[t] = ni;
+          my_total += (unsigned long long)ni;
+        }
+    }
+  for(int o = 16; o > 0; o >>= 1)
+    my_total += __shfl_xor_sync(0xffffffffu, my_total, o);
+  if(lane == 0 && my_total)
+    atomicAdd(total, my_total);
+}
+
+int grid_for(int64_t n, int threads)
+{
+  int64_t b = (n + threads - 1) / threads;
+  if(b > 148 * 16)
+    b = 148 * 16;
+  return (int)(b < 1 ? 1 : b);
+}
+
+void make_w32(const WalkConst &wc, W32Const *w)
+{
+  memset(w, 0, sizeof(*w));
+  w->box       = wc.box;
+  w->half_box  = wc.half_box;
+  w->rcut      = (float)wc.rcut;
+  w->rcut2     = (float)wc.rcut2;
+  w->asmthfac  = (float)wc.asmthfac;
+  w->asmthinv2 = (float)wc.asmthinv2;
+  w->theta2    = (float)(wc.theta * wc.theta);
+  w->erracc    = (float)wc.erracc;
+  w->periodic  = wc.periodic;
+  w->bh        = wc.bh;
+  for(int i = 0; i <= GPUGRAV_MAX_SOFTTYPES; i++)
+    w->soft[i] = (float)wc.soft[i];
+  for(int i = 0; i <= kNtab; i++)
+    {
+      float f0 = wc.tab_force[i], f1 = (i < kNtab) ? wc.tab_force[i + 1] : wc.tab_force[i];
+      float p0 = wc.tab_pot[i], p1 = (i < kNtab) ? wc.tab_pot[i + 1] : wc.tab_pot[i];
+      w->tab[i]  = make_float2(f0, f1 - f0);
+      w->tabp[i] = make_float2(p0, p1 - p0);
+    }
+}
+}  // namespace
+
+#define GG_TRY(x)             \
+  do                          \
+    {                         \
+      cudaError_t _e = (x);   \
+      if(_e != cudaSuccess)   \
+        return _e;            \
+    }                         \
+  while(0)
+
+// breadth-first node layout + particles grouped by parent (built once per tree)
 cudaError_t layout32_stage(gpugrav_ctx *c)
 {
-  (void)c;
-  return cudaErrorNotSupported;
+  const int64_t n = c->n, nn = c->num_nodes;
+  cudaStream_t st = c->stream;
+  GG_TRY(c->g_key.ensure(nn * 8));
+  GG_TRY(c->g_key_alt.ensure(nn * 8));
+  GG_TRY(c->g_val.ensure(nn * 4));
+  GG_TRY(c->g_val_alt.ensure(nn * 4));
+  GG_TRY(c->g_bfs.ensure(nn * 4));
+  GG_TRY(c->g_np.ensure((nn + 1) * 4));
+  GG_TRY(c->g_poff.ensure((nn + 1) * 4));
+  GG_TRY(c->g_sm.ensure(nn * sizeof(double4)));
+  GG_TRY(c->g_rel.ensure(nn * sizeof(float4)));
+  GG_TRY(c->g_kids.ensure(nn * sizeof(int4)));
+  GG_TRY(c->g_pm.ensure(n * sizeof(double4)));
+  GG_TRY(c->g_pst.ensure(n + 16));
+  k_g_keys<<<grid_for(nn, 256), 256, 0, st>>>(nn, c->n_depth.as<uint8_t>(), c->n_dfs.as<int32_t>(), c->g_key.as<uint64_t>(),
+                                               c->g_val.as<int32_t>());
+  size_t tb = 0;
+  GG_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, c->g_key.as<uint64_t>(), c->g_key_alt.as<uint64_t>(),
+                                         c->g_val.as<int32_t>(), c->g_val_alt.as<int32_t>(), (int)nn, 0, 40, st));
+  GG_TRY(c->sort_tmp.ensure(tb));
+  GG_TRY(cub::DeviceRadixSort::SortPairs(c->sort_tmp.p, tb, c->g_key.as<uint64_t>(), c->g_key_alt.as<uint64_t>(),
+                                         c->g_val.as<int32_t>(), c->g_val_alt.as<int32_t>(), (int)nn, 0, 40, st));
+  k_g_rank<<<grid_for(nn, 256), 256, 0, st>>>(nn, n, c->g_val_alt.as<int32_t>(), c->n_suns.as<int32_t>(), c->g_bfs.as<int32_t>(),
+                                               c->g_np.as<int32_t>());
+  tb = 0;
+  GG_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, c->g_np.as<int32_t>(), c->g_poff.as<int32_t>(), (int)nn, st));
+  GG_TRY(c->sort_tmp.ensure(tb));
+  GG_TRY(cub::DeviceScan::ExclusiveSum(c->sort_tmp.p, tb, c->g_np.as<int32_t>(), c->g_poff.as<int32_t>(), (int)nn, st));
+  int *err = c->counters.as<int>() + 13;
+  GG_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
+  k_g_fill<<<grid_for(nn, 256), 256, 0, st>>>(nn, n, c->g_val_alt.as<int32_t>(), c->n_suns.as<int32_t>(), c->g_bfs.as<int32_t>(),
+                                               c->g_poff.as<int32_t>(), c->n_sm.as<double4>(), c->n_cl.as<double4>(),
+                                               c->n_maxsoft.as<uint8_t>(), c->s_pm.as<double4>(), c->s_st.as<uint8_t>(),
+                                               c->g_sm.as<double4>(), c->g_rel.as<float4>(), c->g_kids.as<int4>(),
+                                               c->g_pm.as<double4>(), c->g_pst.as<uint8_t>(), err);
+  GG_TRY(cudaGetLastError());
+  int e = 0;
+  GG_TRY(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  GG_TRY(cudaStreamSynchronize(st));
+  if(e)
+    return cudaErrorUnknown;
+  c->layout32_valid = true;
+  return cudaSuccess;
+}
+
+cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc)
+{
+  if(!c->layout32_valid)
+    GG_TRY(layout32_stage(c));
+  cudaStream_t st = c->stream;
+  const int64_t n = c->n;
+  W32Const w;
+  make_w32(wc, &w);
+  // constants live after the per-warp stacks' bookkeeping in the scratch buffer
+  GG_TRY(c->scratch.ensure(sizeof(W32Const) + 256));
+  GG_TRY(cudaMemcpyAsync(c->scratch.p, &w, sizeof(w), cudaMemcpyHostToDevice, st));
+  int dev = 0, sms = 0, per_sm = 0;
+  GG_TRY(cudaGetDevice(&dev));
+  GG_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  GG_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk32<true>, 32 * kWarps, 0));
+  if(per_sm < 1)
+    per_sm = 1;
+  const int blocks  = sms * per_sm;
+  const int ngroups = (int)((n + 31) / 32);
+  GG_TRY(c->g_stack.ensure((size_t)blocks * kWarps * kStackCap * sizeof(int)));
+  int *work = c->counters.as<int>() + 20;
+  int *err  = c->counters.as<int>() + 14;
+  GG_TRY(cudaMemsetAsync(work, 0, sizeof(int), st));
+  GG_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
+  k_walk32<true><<<blocks, 32 * kWarps, 0, st>>>(c->g_sm.as<double4>(), c->g_rel.as<float4>(), c->g_kids.as<int4>(),
+                                                 c->g_pm.as<double4>(), c->g_pst.as<uint8_t>(), c->s_pm.as<double4>(),
+                                                 c->s_st.as<uint8_t>(), c->oldacc_s.as<float>(), n, ngroups,
+                                                 (const W32Const *)c->scratch.p, c->g_stack.as<int>(), work,
+                                                 c->acc_s.as<double>(), c->pot_s.as<double>(), c->nint_s.as<int32_t>(),
+                                                 (unsigned long long *)(c->counters.as<int>() + 32), err);
+  return cudaGetLastError();
 }
 }  // namespace gg

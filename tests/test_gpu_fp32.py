@@ -1,0 +1,85 @@
+"""The FP32 group walk: accuracy against FP64 direct summation, compared with the
+FP64 parity walk (the reference's own decisions) on the same particles.
+
+The group walk accepts a node only if every target of the group would accept it,
+so its tree-approximation error must not exceed the parity walk's; FP32
+arithmetic with FP64 separations adds a rounding error far below 1e-4."""
+import numpy as np
+import pytest
+
+from arepo_b200 import _lib as L
+from arepo_b200 import ics
+from arepo_b200.gravity import GravityTree
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(ic, precision, targets):
+    prm = ics.params_for(ic, precision=precision)
+    with GravityTree(prm) as t:
+        acc, pot, ni, oldacc = t.compute_grav_accelerations(ic["pos"], ic["mass"], ic["softtype"])
+        d_cut, _ = t.direct(targets, cut=True)
+    return acc, pot, ni, d_cut
+
+
+def _err(acc, ref):
+    dn = np.linalg.norm(ref, axis=1)
+    e = np.linalg.norm(acc - ref, axis=1)
+    scale = np.sqrt(np.mean(dn * dn))
+    return float(np.sqrt(np.mean((e / np.maximum(dn, 1e-300)) ** 2))), float(np.sqrt(np.mean((e / scale) ** 2)))
+
+
+CASES = {
+    "grid32": lambda: ics.grid_box(n1=32, seed=1001, pmgrid=64),
+    "hernquist": lambda: ics.hernquist(1 << 16, seed=1002),
+    "zoom": lambda: ics.zoom_box(log2_half=15, seed=1004, pmgrid=128),
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_fp32_walk_at_least_as_accurate_as_parity_walk(name, cuda_lib):
+    ic = CASES[name]()
+    n = len(ic["mass"])
+    tg = np.sort(np.random.default_rng(5).choice(n, 2048, replace=False))
+    a64, _, n64, d = _run(ic, L.PREC_FP64, tg)
+    a32, _, n32, _ = _run(ic, L.PREC_FP32, tg)
+    rel64, glob64 = _err(a64[tg], d)
+    rel32, glob32 = _err(a32[tg], d)
+    # conservative group decisions: no less accurate than per-target decisions (FP32 rounding slack)
+    assert glob32 <= glob64 * 1.02 + 2e-5, (glob32, glob64)
+    assert rel32 <= rel64 * 1.02 + 2e-5, (rel32, rel64)
+    assert n32.sum() >= n64.sum()
+    assert np.all(np.isfinite(a32))
+
+
+def test_fp32_walk_matches_fp64_walk_with_tight_criterion(cuda_lib):
+    """With a very tight relative criterion both walks converge to the direct sum; FP32
+    rounding with FP64 separations stays below 1e-5 relative."""
+    ic = ics.grid_box(n1=24, seed=3, pmgrid=48)
+    prm64 = ics.params_for(ic, precision=L.PREC_FP64, err_tol_force_acc=1e-7)
+    prm32 = ics.params_for(ic, precision=L.PREC_FP32, err_tol_force_acc=1e-7)
+    with GravityTree(prm64) as t:
+        a64, _, _, _ = t.compute_grav_accelerations(ic["pos"], ic["mass"], ic["softtype"])
+    with GravityTree(prm32) as t:
+        a32, p32, _, _ = t.compute_grav_accelerations(ic["pos"], ic["mass"], ic["softtype"])
+    scale = np.sqrt(np.mean(np.sum(a64 * a64, axis=1)))
+    err = np.linalg.norm(a32 - a64, axis=1) / scale
+    assert np.sqrt(np.mean(err ** 2)) < 1e-5
+    assert np.all(np.isfinite(p32))
+
+
+@pytest.mark.parametrize("name", ["grid16_pm", "hernquist2048_iso", "mix1500_pm"])
+def test_fp32_walk_on_golden_inputs(name, cuda_lib):
+    g = load_golden(name)
+    p = g["params"]
+    ic = dict(pos=g["pos"], mass=g["mass"], softtype=g["softtype"], periodic=p["periodic"], box=p["box"],
+              asmth=p["asmth"], rcut=p["rcut"], softening=tuple(p["softening"]))
+    tg = np.arange(len(g["mass"]))
+    a64, _, _, d = _run(ic, L.PREC_FP64, tg)
+    a32, _, _, _ = _run(ic, L.PREC_FP32, tg)
+    _, glob64 = _err(a64, d)
+    _, glob32 = _err(a32, d)
+    assert glob32 <= glob64 * 1.02 + 2e-5
+    # and the FP64 path is the reference's own result
+    assert np.array_equal(a64[g["order"]], g["acc1"])
