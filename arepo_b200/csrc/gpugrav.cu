@@ -493,6 +493,7 @@ int32_t gpugrav_walk(gpugrav_ctx *c, const float *oldacc, double *acc, double *p
     return fail(c, GPUGRAV_ERR_OOM, "gpugrav_walk: device allocation");
   WalkConst wc;
   make_walk_const(c->prm, &wc);
+  c->want_pot = (pot != nullptr);
   CK(cudaMemcpyAsync(c->wconst.p, &wc, sizeof(wc), cudaMemcpyHostToDevice, st), "walk constants");
   cudaEventRecord(c->ev[7], st);
   const float *old_dev = nullptr;

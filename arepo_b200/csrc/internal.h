@@ -117,6 +117,7 @@ struct gpugrav_ctx
   gg::DevBuf g_pm, g_pst;                     // particles in parent order: (x, y, z, m) double4; softening type
   gg::DevBuf g_stack;                         // per-warp traversal stacks
   bool layout32_valid = false;
+  bool want_pot       = true;  // potential requested by the current walk call
   gg::DevBuf acc_s, pot_s, nint_s, oldacc_s, oldacc_in;  // per target (sorted), inputs
   gg::DevBuf out_acc, out_pot, out_nint;      // caller order staging for host copies
   gg::DevBuf scratch;                         // reductions

@@ -171,7 +171,21 @@ __device__ __forceinline__ int wscan_incl(int v, int lane)
   return v;
 }
 
-template <bool POT>
+// Table index without conversion instructions: adding 1.5 * 2^23 leaves round(te - 0.5)
+// (= floor(te) up to ties, where both neighbours give the same interpolated value) in the
+// low mantissa bits.
+__device__ __forceinline__ float2 tab_lookup(const float2 *tab, float te, float &tw)
+{
+  const float tb0 = (te - 0.5f) + 12582912.0f;
+  const int ti    = __float_as_int(tb0) - 0x4B400000;
+  tw              = te - (tb0 - 12582912.0f);
+  return tab[ti];
+}
+
+// One lane's target against `nl` list entries.  Entries beyond Rcut of this target
+// (periodic) are masked, not branched around; the softening branch is taken only inside
+// the spline support.
+template <bool PERIODIC, bool POT>
 __device__ __forceinline__ void evaluate(const float4 *__restrict__ LP, const float *__restrict__ LH, int nl, float xr, float yr,
                                          float zr, float hi, const W32Const &w, float &ax, float &ay, float &az, float &pot,
                                          int &ni)
@@ -179,36 +193,36 @@ __device__ __forceinline__ void evaluate(const float4 *__restrict__ LP, const fl
 #pragma unroll 4
   for(int j = 0; j < nl; j++)
     {
-      const float4 e = LP[j];
-      const float hj = LH[j];
-      const float dx = e.x - xr, dy = e.y - yr, dz = e.z - zr;
-      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      if(w.periodic && !(r2 < w.rcut2))
-        continue;
+      const float4 e   = LP[j];
+      const float hj   = LH[j];
+      const float dx   = e.x - xr, dy = e.y - yr, dz = e.z - zr;
+      const float r2   = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
       const float hmax = fmaxf(hi, hj);
       const float rinv = (r2 > 0.0f) ? rsqrtf(r2) : 0.0f;
       const float r    = r2 * rinv;
+      bool in          = true;
       float ff = 0.0f, fpt = 0.0f;
-      if(w.periodic)
+      if(PERIODIC)
         {
-          const float te = r * w.asmthfac;
-          int ti         = (int)te;
-          ti             = ti < kNtab - 1 ? ti : kNtab - 1;
-          const float tw = te - (float)ti;
-          const float2 tb = w.tab[ti];
-          ff             = fmaf(tw, tb.y, tb.x);
+          in = r2 < w.rcut2;
+          // inside Rcut te < NTAB; the clamp (just below NTAB, so the last interval keeps its
+          // interpolation) only bounds the index of masked entries beyond Rcut
+          const float te = fminf(r * w.asmthfac, (float)kNtab - 0.0001f);
+          float tw;
+          const float2 tb = tab_lookup(w.tab, te, tw);
+          ff              = fmaf(tw, tb.y, tb.x);
           if(POT)
             {
-              const float2 tp = w.tabp[ti];
-              fpt             = fmaf(tw, tp.y, tp.x);
+              float tw2;
+              const float2 tp = tab_lookup(w.tabp, te, tw2);
+              fpt             = fmaf(tw2, tp.y, tp.x);
             }
         }
       float fac, wp = 0.0f;
       if(r >= hmax)
         {
-          const float rinv2 = rinv * rinv;
-          fac               = rinv2 * rinv;
-          if(w.periodic)
+          fac = rinv * rinv * rinv;
+          if(PERIODIC)
             {
               fac = fmaf(rinv * ff, w.asmthinv2, fac);
               if(POT)
@@ -236,27 +250,25 @@ __device__ __forceinline__ void evaluate(const float4 *__restrict__ LP, const fl
               if(POT)
                 wp = h_inv * (SF13 + SF14 / u + u2 * (SF1 + u * (SF15 + u * (SF16 + SF17 * u))));
             }
-          if(w.periodic && r > 0.0f)
+          if(PERIODIC && r > 0.0f)
             {
               fac = fmaf(rinv * ff, w.asmthinv2, fac);
               if(POT)
                 wp = fmaf(rinv, fpt + 1.0f, wp);
             }
         }
-      if(e.w != 0.0f)
-        {
-          const float fm = fac * e.w;
-          ax             = fmaf(dx, fm, ax);
-          ay             = fmaf(dy, fm, ay);
-          az             = fmaf(dz, fm, az);
-          if(POT)
-            pot = fmaf(e.w, wp, pot);
-          ni++;
-        }
+      const float m  = in ? e.w : 0.0f;
+      const float fm = fac * m;
+      ax             = fmaf(dx, fm, ax);
+      ay             = fmaf(dy, fm, ay);
+      az             = fmaf(dz, fm, az);
+      if(POT)
+        pot = fmaf(m, wp, pot);
+      ni += (m != 0.0f) ? 1 : 0;
     }
 }
 
-template <bool POT>
+template <bool PERIODIC, bool POT>
 __global__ void __launch_bounds__(32 * kWarps) k_walk32(const double4 *__restrict__ g_sm, const float4 *__restrict__ g_rel,
                                                         const int4 *__restrict__ g_kids, const double4 *__restrict__ g_pm,
                                                         const uint8_t *__restrict__ g_pst, const double4 *__restrict__ tpm,
@@ -290,19 +302,19 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk32(const double4 *__restric
       grp = __shfl_sync(0xffffffffu, grp, 0);
       if(grp >= ngroups)
         break;
-      const int64_t t0   = (int64_t)grp * 32;
-      const int64_t t    = t0 + lane;
-      const bool valid   = t < n;
-      const int64_t tt   = valid ? t : t0;
-      const double4 p    = tpm[tt];
-      // group box (FP64), centre g, half extent
+      const int64_t t0 = (int64_t)grp * 32;
+      const int64_t t  = t0 + lane;
+      const bool valid = t < n;
+      const int64_t tt = valid ? t : t0;
+      const double4 p  = tpm[tt];
+      // group box (FP64), centre g, half extent (rounded up)
       const double mnx = wmin(p.x), mxx = wmax(p.x), mny = wmin(p.y), mxy = wmax(p.y), mnz = wmin(p.z), mxz = wmax(p.z);
       const double gx = 0.5 * (mnx + mxx), gy = 0.5 * (mny + mxy), gz = 0.5 * (mnz + mxz);
       const float ex = (float)(0.5 * (mxx - mnx)) * 1.000001f, ey = (float)(0.5 * (mxy - mny)) * 1.000001f,
                   ez = (float)(0.5 * (mxz - mnz)) * 1.000001f;
       const float xr = (float)(p.x - gx), yr = (float)(p.y - gy), zr = (float)(p.z - gz);
-      const float hi = w.soft[tst[tt]];
-      const float h_min = wminf(hi);
+      const float hi       = w.soft[tst[tt]];
+      const float h_min    = wminf(hi);
       const float aold_min = wminf(w.erracc * oldacc[tt]);
 
       double dax = 0, day = 0, daz = 0, dpot = 0;
@@ -339,7 +351,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk32(const double4 *__restric
                   const float m  = (float)sm.w;
                   hj             = w.soft[kd.w];
                   bool prune     = false;
-                  if(w.periodic)
+                  if(PERIODIC)
                     {
                       const float eff = w.rcut + 0.5f * L;
                       prune = (fabsf(cx) - ex > eff) || (fabsf(cy) - ey > eff) || (fabsf(cz) - ez > eff);
@@ -366,8 +378,9 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk32(const double4 *__restric
                           nc     = kd.z & 15;
                           np     = (kd.z >> 4) & 15;
                         }
-                      else
+                      else if(!PERIODIC || rmin2 < w.rcut2)
                         {
+                          // accepted; a node whose CoM is beyond Rcut of every target contributes nothing
                           action = 1;
                           entry  = make_float4(sx, sy, sz, m);
                         }
@@ -383,21 +396,53 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk32(const double4 *__restric
               LH[pos]       = hj;
             }
           nl += __popc(am);
-          // particles of opened nodes -> list
+          // particles of opened nodes -> list, one particle per lane per round; particles beyond
+          // Rcut of the whole group are dropped
           const int npx  = (action == 2) ? np : 0;
           const int pinc = wscan_incl(npx, lane);
           const int ptot = __shfl_sync(0xffffffffu, pinc, 31);
-          {
-            const int pb = nl + pinc - npx;
-            for(int q = 0; q < npx; q++)
-              {
-                const double4 pp = g_pm[fp + q];
-                LP[pb + q] = make_float4((float)wrapd(pp.x - gx, w), (float)wrapd(pp.y - gy, w), (float)wrapd(pp.z - gz, w),
-                                         (float)pp.w);
-                LH[pb + q] = w.soft[g_pst[fp + q]];
-              }
-          }
-          nl += ptot;
+          const int pexc = pinc - npx;
+          for(int q0 = 0; q0 < ptot; q0 += 32)
+            {
+              const int q = q0 + lane;
+              int L = 0;  // owner lane: number of lanes whose inclusive prefix is <= q
+#pragma unroll
+              for(int s = 16; s >= 1; s >>= 1)
+                {
+                  const int v = __shfl_sync(0xffffffffu, pinc, L + s - 1);
+                  if(v <= q)
+                    L += s;
+                }
+              L              = L < 31 ? L : 31;
+              const int ofp  = __shfl_sync(0xffffffffu, fp, L);
+              const int oexc = __shfl_sync(0xffffffffu, pexc, L);
+              bool keep      = false;
+              float4 pe      = make_float4(0, 0, 0, 0);
+              float ph       = 0;
+              if(q < ptot)
+                {
+                  const int pi     = ofp + (q - oexc);
+                  const double4 pp = g_pm[pi];
+                  pe = make_float4((float)wrapd(pp.x - gx, w), (float)wrapd(pp.y - gy, w), (float)wrapd(pp.z - gz, w),
+                                   (float)pp.w);
+                  ph   = w.soft[g_pst[pi]];
+                  keep = pp.w != 0.0;
+                  if(PERIODIC)
+                    {
+                      const float dmx = fmaxf(fabsf(pe.x) - ex, 0.0f), dmy = fmaxf(fabsf(pe.y) - ey, 0.0f),
+                                  dmz = fmaxf(fabsf(pe.z) - ez, 0.0f);
+                      keep = keep && (dmx * dmx + dmy * dmy + dmz * dmz < w.rcut2);
+                    }
+                }
+              const unsigned km = __ballot_sync(0xffffffffu, keep);
+              if(keep)
+                {
+                  const int pos = nl + __popc(km & lt_mask);
+                  LP[pos]       = pe;
+                  LH[pos]       = ph;
+                }
+              nl += __popc(km);
+            }
           // node children of opened nodes -> stack (contiguous in breadth-first order)
           const int ncx  = (action == 2) ? nc : 0;
           const int cinc = wscan_incl(ncx, lane);
@@ -414,7 +459,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk32(const double4 *__restric
           __syncwarp();
           if(nl >= kEvalAt)
             {
-              evaluate<POT>(LP, LH, nl, xr, yr, zr, hi, w, ax, ay, az, pt, ni);
+              evaluate<PERIODIC, POT>(LP, LH, nl, xr, yr, zr, hi, w, ax, ay, az, pt, ni);
               dax += ax;
               day += ay;
               daz += az;
@@ -426,7 +471,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk32(const double4 *__restric
         }
       if(nl > 0)
         {
-          evaluate<POT>(LP, LH, nl, xr, yr, zr, hi, w, ax, ay, az, pt, ni);
+          evaluate<PERIODIC, POT>(LP, LH, nl, xr, yr, zr, hi, w, ax, ay, az, pt, ni);
           dax += ax;
           day += ay;
           daz += az;
@@ -554,7 +599,10 @@ cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc)
   int dev = 0, sms = 0, per_sm = 0;
   GG_TRY(cudaGetDevice(&dev));
   GG_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  GG_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk32<true>, 32 * kWarps, 0));
+  const bool periodic = wc.periodic != 0;
+  const bool pot      = c->want_pot;
+  auto kern = periodic ? (pot ? k_walk32<true, true> : k_walk32<true, false>) : (pot ? k_walk32<false, true> : k_walk32<false, false>);
+  GG_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * kWarps, 0));
   if(per_sm < 1)
     per_sm = 1;
   const int blocks  = sms * per_sm;
@@ -563,13 +611,11 @@ cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc)
   int *work = c->counters.as<int>() + 20;
   int *err  = c->counters.as<int>() + 14;
   GG_TRY(cudaMemsetAsync(work, 0, sizeof(int), st));
-  GG_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
-  k_walk32<true><<<blocks, 32 * kWarps, 0, st>>>(c->g_sm.as<double4>(), c->g_rel.as<float4>(), c->g_kids.as<int4>(),
-                                                 c->g_pm.as<double4>(), c->g_pst.as<uint8_t>(), c->s_pm.as<double4>(),
-                                                 c->s_st.as<uint8_t>(), c->oldacc_s.as<float>(), n, ngroups,
-                                                 (const W32Const *)c->scratch.p, c->g_stack.as<int>(), work,
-                                                 c->acc_s.as<double>(), c->pot_s.as<double>(), c->nint_s.as<int32_t>(),
-                                                 (unsigned long long *)(c->counters.as<int>() + 32), err);
+  kern<<<blocks, 32 * kWarps, 0, st>>>(c->g_sm.as<double4>(), c->g_rel.as<float4>(), c->g_kids.as<int4>(), c->g_pm.as<double4>(),
+                                       c->g_pst.as<uint8_t>(), c->s_pm.as<double4>(), c->s_st.as<uint8_t>(),
+                                       c->oldacc_s.as<float>(), n, ngroups, (const W32Const *)c->scratch.p, c->g_stack.as<int>(),
+                                       work, c->acc_s.as<double>(), c->pot_s.as<double>(), c->nint_s.as<int32_t>(),
+                                       (unsigned long long *)(c->counters.as<int>() + 32), err);
   return cudaGetLastError();
 }
 }  // namespace gg

@@ -91,14 +91,15 @@ class GravityTree:
             self._check(self.lib.gpugrav_build(self._ctx, None, 0))
         return self.tree_info().num_nodes
 
-    def gravity_tree(self, oldacc=None, acc=None, pot=None, ninter=None, mem: int = L.MEM_HOST):
+    def gravity_tree(self, oldacc=None, acc=None, pot=None, ninter=None, mem: int = L.MEM_HOST, want_pot: bool = True):
         """Accelerations (without G), potentials and interaction counts for every particle,
-        in the caller's order. With mem=MEM_HOST numpy outputs are allocated when not given."""
+        in the caller's order. With mem=MEM_HOST numpy outputs are allocated when not given;
+        want_pot=False skips the potential (EVALPOTENTIAL off)."""
         n = self.n
         if mem == L.MEM_HOST:
             if acc is None:
                 acc = np.empty((n, 3), np.float64)
-            if pot is None:
+            if pot is None and want_pot:
                 pot = np.empty(n, np.float64)
             if ninter is None:
                 ninter = np.empty(n, np.int32)

@@ -83,3 +83,15 @@ def test_fp32_walk_on_golden_inputs(name, cuda_lib):
     assert glob32 <= glob64 * 1.02 + 2e-5
     # and the FP64 path is the reference's own result
     assert np.array_equal(a64[g["order"]], g["acc1"])
+
+
+def test_fp32_walk_without_potential_gives_same_forces(cuda_lib):
+    ic = ics.zoom_box(log2_half=13, seed=11, pmgrid=64)
+    prm = ics.params_for(ic, precision=L.PREC_FP32)
+    with GravityTree(prm) as t:
+        t.domain_decomposition(ic["pos"], ic["mass"], ic["softtype"])
+        t.construct_forcetree()
+        a1, p1, n1 = t.gravity_tree()
+        a2, p2, n2 = t.gravity_tree(want_pot=False)
+    assert p2 is None and np.all(np.isfinite(p1))
+    assert np.array_equal(a1, a2) and np.array_equal(n1, n2)
