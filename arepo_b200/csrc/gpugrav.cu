@@ -8,6 +8,7 @@
 // nothing in the library exits.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -274,6 +275,8 @@ int32_t gpugrav_create(gpugrav_ctx **out, int32_t device, const gpugrav_params *
     return GPUGRAV_ERR_OOM;
   c->device = device;
   c->prm    = *p;
+  if(const char *e = getenv("GPUGRAV_WALK32_TPL"))
+    c->walk32_tpl = atoi(e) == 1 ? 1 : 2;
   DeviceGuard g(device);
   if(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     {

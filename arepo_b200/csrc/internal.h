@@ -118,6 +118,7 @@ struct gpugrav_ctx
   gg::DevBuf g_stack;                         // per-warp traversal stacks
   bool layout32_valid = false;
   bool want_pot       = true;  // potential requested by the current walk call
+  int walk32_tpl      = 1;     // targets per lane of the FP32 walk (1 or 2; GPUGRAV_WALK32_TPL)
   gg::DevBuf acc_s, pot_s, nint_s, oldacc_s, oldacc_in;  // per target (sorted), inputs
   gg::DevBuf out_acc, out_pot, out_nint;      // caller order staging for host copies
   gg::DevBuf scratch;                         // reductions

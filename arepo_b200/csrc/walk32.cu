@@ -29,9 +29,24 @@ namespace gg
 {
 namespace
 {
-constexpr int kWarps    = 4;      // warps per block
-constexpr int kListCap  = 448;    // interaction list entries per warp
-constexpr int kEvalAt   = 160;    // evaluate once this many entries are queued
+#ifndef GG_W32_WARPS
+#define GG_W32_WARPS 4
+#endif
+#ifndef GG_W32_EVAL_AT
+#define GG_W32_EVAL_AT 192
+#endif
+#ifndef GG_W32_UNROLL
+#define GG_W32_UNROLL 4
+#endif
+constexpr int kWarps   = GG_W32_WARPS;    // warps per block
+constexpr int kEvalAt  = GG_W32_EVAL_AT;  // evaluate once this many entries are queued
+constexpr int kUnroll  = GG_W32_UNROLL;   // list entries in flight per lane in the evaluation loop
+#ifndef GG_W32_MINBLOCKS
+#define GG_W32_MINBLOCKS 6
+#endif
+// capacity: accepted nodes (<= 32) join a list holding fewer than kEvalAt entries; particles are
+// added at most 32 per round and the list is evaluated first whenever a round could overflow it
+constexpr int kListCap = kEvalAt + 64;
 constexpr int kStackCap = 16384;  // traversal stack entries per warp (global memory)
 
 #define SF1 10.666666666667f
@@ -182,94 +197,144 @@ __device__ __forceinline__ float2 tab_lookup(const float2 *tab, float te, float 
   return tab[ti];
 }
 
-// One lane's target against `nl` list entries.  Entries beyond Rcut of this target
-// (periodic) are masked, not branched around; the softening branch is taken only inside
-// the spline support.
-template <bool PERIODIC, bool POT>
-__device__ __forceinline__ void evaluate(const float4 *__restrict__ LP, const float *__restrict__ LH, int nl, float xr, float yr,
-                                         float zr, float hi, const W32Const &w, float &ax, float &ay, float &az, float &pot,
-                                         int &ni)
+// Per-target state of a lane (targets per lane: TPL).
+struct Tgt
 {
-#pragma unroll 4
-  for(int j = 0; j < nl; j++)
+  float x, y, z, h;         // position relative to the group centre, softening
+  float ax, ay, az, pot;    // FP32 partial sums of the current list batch
+  double dax, day, daz, dpot;  // batch partials accumulated in FP64
+  int ni;
+};
+
+// One target against one list entry.  An entry beyond Rcut of this target (periodic) is
+// masked, not branched around; the softening branch is taken only inside the spline support.
+template <bool PERIODIC, bool POT>
+__device__ __forceinline__ void interact(const float4 e, const float hj, Tgt &T, const W32Const &w)
+{
+  const float dx   = e.x - T.x, dy = e.y - T.y, dz = e.z - T.z;
+  const float r2   = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  const float hmax = fmaxf(T.h, hj);
+  // a zero separation (the target itself) gives a huge rinv but r = 0: the spline branch,
+  // whose periodic term is skipped at r = 0, handles it
+  const float rinv = rsqrtf(fmaxf(r2, 1.0e-30f));
+  const float r    = r2 * rinv;
+  bool in          = true;
+  float ff = 0.0f, fpt = 0.0f;
+  if(PERIODIC)
     {
-      const float4 e   = LP[j];
-      const float hj   = LH[j];
-      const float dx   = e.x - xr, dy = e.y - yr, dz = e.z - zr;
-      const float r2   = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      const float hmax = fmaxf(hi, hj);
-      const float rinv = (r2 > 0.0f) ? rsqrtf(r2) : 0.0f;
-      const float r    = r2 * rinv;
-      bool in          = true;
-      float ff = 0.0f, fpt = 0.0f;
+      in = r2 < w.rcut2;
+      // inside Rcut te < NTAB; the clamp (just below NTAB, so the last interval keeps its
+      // interpolation) only bounds the index of masked entries beyond Rcut
+      const float te = fminf(r * w.asmthfac, (float)kNtab - 0.0001f);
+      float tw;
+      const float2 tb = tab_lookup(w.tab, te, tw);
+      ff              = fmaf(tw, tb.y, tb.x);
+      if(POT)
+        {
+          float tw2;
+          const float2 tp = tab_lookup(w.tabp, te, tw2);
+          fpt             = fmaf(tw2, tp.y, tp.x);
+        }
+    }
+  float fac, wp = 0.0f;
+  if(r >= hmax)
+    {
+      fac = rinv * rinv * rinv;
       if(PERIODIC)
         {
-          in = r2 < w.rcut2;
-          // inside Rcut te < NTAB; the clamp (just below NTAB, so the last interval keeps its
-          // interpolation) only bounds the index of masked entries beyond Rcut
-          const float te = fminf(r * w.asmthfac, (float)kNtab - 0.0001f);
-          float tw;
-          const float2 tb = tab_lookup(w.tab, te, tw);
-          ff              = fmaf(tw, tb.y, tb.x);
+          fac = fmaf(rinv * ff, w.asmthinv2, fac);
           if(POT)
-            {
-              float tw2;
-              const float2 tp = tab_lookup(w.tabp, te, tw2);
-              fpt             = fmaf(tw2, tp.y, tp.x);
-            }
+            wp = rinv * fpt;
         }
-      float fac, wp = 0.0f;
-      if(r >= hmax)
+      else if(POT)
+        wp = -rinv;
+    }
+  else
+    {
+      const float h_inv  = 1.0f / hmax;
+      const float h3_inv = h_inv * h_inv * h_inv;
+      const float u      = r * h_inv;
+      const float u2     = u * u;
+      if(u < 0.5f)
         {
-          fac = rinv * rinv * rinv;
-          if(PERIODIC)
-            {
-              fac = fmaf(rinv * ff, w.asmthinv2, fac);
-              if(POT)
-                wp = rinv * fpt;
-            }
-          else if(POT)
-            wp = -rinv;
+          fac = h3_inv * fmaf(u2, fmaf(SF2, u, SF3), SF1);
+          if(POT)
+            wp = h_inv * fmaf(u2, fmaf(u2, fmaf(SF6, u, SF7), SF5), SF4);
         }
       else
         {
-          const float h_inv  = 1.0f / hmax;
-          const float h3_inv = h_inv * h_inv * h_inv;
-          const float u      = r * h_inv;
-          const float u2     = u * u;
-          if(u < 0.5f)
-            {
-              fac = h3_inv * fmaf(u2, fmaf(SF2, u, SF3), SF1);
-              if(POT)
-                wp = h_inv * fmaf(u2, fmaf(u2, fmaf(SF6, u, SF7), SF5), SF4);
-            }
-          else
-            {
-              const float u3 = u2 * u;
-              fac = h3_inv * (SF8 + SF9 * u + SF10 * u2 + SF11 * u3 + SF12 / u3);
-              if(POT)
-                wp = h_inv * (SF13 + SF14 / u + u2 * (SF1 + u * (SF15 + u * (SF16 + SF17 * u))));
-            }
-          if(PERIODIC && r > 0.0f)
-            {
-              fac = fmaf(rinv * ff, w.asmthinv2, fac);
-              if(POT)
-                wp = fmaf(rinv, fpt + 1.0f, wp);
-            }
+          const float u3 = u2 * u;
+          fac = h3_inv * (SF8 + SF9 * u + SF10 * u2 + SF11 * u3 + SF12 / u3);
+          if(POT)
+            wp = h_inv * (SF13 + SF14 / u + u2 * (SF1 + u * (SF15 + u * (SF16 + SF17 * u))));
         }
-      const float m  = in ? e.w : 0.0f;
-      const float fm = fac * m;
-      ax             = fmaf(dx, fm, ax);
-      ay             = fmaf(dy, fm, ay);
-      az             = fmaf(dz, fm, az);
-      if(POT)
-        pot = fmaf(m, wp, pot);
-      ni += (m != 0.0f) ? 1 : 0;
+      if(PERIODIC && r > 0.0f)
+        {
+          fac = fmaf(rinv * ff, w.asmthinv2, fac);
+          if(POT)
+            wp = fmaf(rinv, fpt + 1.0f, wp);
+        }
+    }
+  const float m  = in ? e.w : 0.0f;
+  const float fm = fac * m;
+  T.ax           = fmaf(dx, fm, T.ax);
+  T.ay           = fmaf(dy, fm, T.ay);
+  T.az           = fmaf(dz, fm, T.az);
+  if(POT)
+    T.pot = fmaf(m, wp, T.pot);
+  T.ni += in ? 1 : 0;  // list entries all have mass != 0
+}
+
+// The lane's TPL targets against `nl` list entries (each entry read once for all of them),
+// then the batch partials are folded into the FP64 sums.
+#ifdef GG_WALK32_STATS
+}  // namespace
+// measurement build only: [0] list entries evaluated per lane, [1] node tests, [2] particle candidates,
+// [3] groups
+__device__ unsigned long long g_walk_stats[4];
+namespace
+{
+#define WALK_STAT(i, v)                       \
+  do                                          \
+    {                                         \
+      if((threadIdx.x & 31) == 0)             \
+        atomicAdd(&g_walk_stats[i], (unsigned long long)(v)); \
+    }                                         \
+  while(0)
+#else
+#define WALK_STAT(i, v) \
+  do                    \
+    {                   \
+    }                   \
+  while(0)
+#endif
+
+template <bool PERIODIC, bool POT, int TPL>
+__device__ __forceinline__ void evaluate(const float4 *__restrict__ LP, const float *__restrict__ LH, int nl, Tgt (&T)[TPL],
+                                         const W32Const &w)
+{
+#pragma unroll kUnroll
+  for(int j = 0; j < nl; j++)
+    {
+      const float4 e = LP[j];
+      const float hj = LH[j];
+#pragma unroll
+      for(int k = 0; k < TPL; k++)
+        interact<PERIODIC, POT>(e, hj, T[k], w);
+    }
+#pragma unroll
+  for(int k = 0; k < TPL; k++)
+    {
+      T[k].dax += T[k].ax;
+      T[k].day += T[k].ay;
+      T[k].daz += T[k].az;
+      T[k].dpot += T[k].pot;
+      T[k].ax = T[k].ay = T[k].az = T[k].pot = 0.0f;
     }
 }
 
-template <bool PERIODIC, bool POT>
-__global__ void __launch_bounds__(32 * kWarps) k_walk32(const double4 *__restrict__ g_sm, const float4 *__restrict__ g_rel,
+template <bool PERIODIC, bool POT, int TPL>
+__global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const double4 *__restrict__ g_sm, const float4 *__restrict__ g_rel,
                                                         const int4 *__restrict__ g_kids, const double4 *__restrict__ g_pm,
                                                         const uint8_t *__restrict__ g_pst, const double4 *__restrict__ tpm,
                                                         const uint8_t *__restrict__ tst, const float *__restrict__ oldacc,
@@ -302,24 +367,44 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk32(const double4 *__restric
       grp = __shfl_sync(0xffffffffu, grp, 0);
       if(grp >= ngroups)
         break;
-      const int64_t t0 = (int64_t)grp * 32;
-      const int64_t t  = t0 + lane;
-      const bool valid = t < n;
-      const int64_t tt = valid ? t : t0;
-      const double4 p  = tpm[tt];
+      WALK_STAT(3, 1);
+      // group of 32*TPL consecutive targets; lane holds targets t0 + lane + 32k
+      const int64_t t0 = (int64_t)grp * 32 * TPL;
+      double4 p[TPL];
+      double mnx = 1e300, mxx = -1e300, mny = 1e300, mxy = -1e300, mnz = 1e300, mxz = -1e300;
+      float hmin_l = 3.0e38f, amin_l = 3.0e38f;
+#pragma unroll
+      for(int k = 0; k < TPL; k++)
+        {
+          const int64_t t  = t0 + lane + 32 * k;
+          const int64_t tt = t < n ? t : t0;  // idle slots repeat the group's first target
+          p[k]             = tpm[tt];
+          mnx = fmin(mnx, p[k].x), mxx = fmax(mxx, p[k].x);
+          mny = fmin(mny, p[k].y), mxy = fmax(mxy, p[k].y);
+          mnz = fmin(mnz, p[k].z), mxz = fmax(mxz, p[k].z);
+          hmin_l = fminf(hmin_l, w.soft[tst[tt]]);
+          amin_l = fminf(amin_l, w.erracc * oldacc[tt]);
+        }
       // group box (FP64), centre g, half extent (rounded up)
-      const double mnx = wmin(p.x), mxx = wmax(p.x), mny = wmin(p.y), mxy = wmax(p.y), mnz = wmin(p.z), mxz = wmax(p.z);
+      mnx = wmin(mnx), mxx = wmax(mxx), mny = wmin(mny), mxy = wmax(mxy), mnz = wmin(mnz), mxz = wmax(mxz);
       const double gx = 0.5 * (mnx + mxx), gy = 0.5 * (mny + mxy), gz = 0.5 * (mnz + mxz);
       const float ex = (float)(0.5 * (mxx - mnx)) * 1.000001f, ey = (float)(0.5 * (mxy - mny)) * 1.000001f,
                   ez = (float)(0.5 * (mxz - mnz)) * 1.000001f;
-      const float xr = (float)(p.x - gx), yr = (float)(p.y - gy), zr = (float)(p.z - gz);
-      const float hi       = w.soft[tst[tt]];
-      const float h_min    = wminf(hi);
-      const float aold_min = wminf(w.erracc * oldacc[tt]);
+      const float h_min    = wminf(hmin_l);
+      const float aold_min = wminf(amin_l);
+      Tgt T[TPL];
+#pragma unroll
+      for(int k = 0; k < TPL; k++)
+        {
+          const int64_t t  = t0 + lane + 32 * k;
+          const int64_t tt = t < n ? t : t0;
+          T[k].x = (float)(p[k].x - gx), T[k].y = (float)(p[k].y - gy), T[k].z = (float)(p[k].z - gz);
+          T[k].h  = w.soft[tst[tt]];
+          T[k].ax = T[k].ay = T[k].az = T[k].pot = 0.0f;
+          T[k].dax = T[k].day = T[k].daz = T[k].dpot = 0.0;
+          T[k].ni = 0;
+        }
 
-      double dax = 0, day = 0, daz = 0, dpot = 0;
-      float ax = 0, ay = 0, az = 0, pt = 0;
-      int ni = 0;
       int nl = 0, sp = 1;
       if(lane == 0)
         stack[0] = 0;  // root
@@ -329,6 +414,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk32(const double4 *__restric
         {
           const int take = sp < 32 ? sp : 32;
           sp -= take;
+          WALK_STAT(1, take);
           int node = -1;
           if(lane < take)
             node = stack[sp + lane];
@@ -402,8 +488,15 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk32(const double4 *__restric
           const int pinc = wscan_incl(npx, lane);
           const int ptot = __shfl_sync(0xffffffffu, pinc, 31);
           const int pexc = pinc - npx;
+          WALK_STAT(2, ptot);
           for(int q0 = 0; q0 < ptot; q0 += 32)
             {
+              if(nl + 32 > kListCap)
+                {
+                  evaluate<PERIODIC, POT, TPL>(LP, LH, nl, T, w);
+                  nl = 0;
+                  __syncwarp();
+                }
               const int q = q0 + lane;
               int L = 0;  // owner lane: number of lanes whose inclusive prefix is <= q
 #pragma unroll
@@ -459,34 +552,32 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk32(const double4 *__restric
           __syncwarp();
           if(nl >= kEvalAt)
             {
-              evaluate<PERIODIC, POT>(LP, LH, nl, xr, yr, zr, hi, w, ax, ay, az, pt, ni);
-              dax += ax;
-              day += ay;
-              daz += az;
-              dpot += pt;
-              ax = ay = az = pt = 0;
+              WALK_STAT(0, nl);
+              evaluate<PERIODIC, POT, TPL>(LP, LH, nl, T, w);
               nl = 0;
               __syncwarp();
             }
         }
       if(nl > 0)
         {
-          evaluate<PERIODIC, POT>(LP, LH, nl, xr, yr, zr, hi, w, ax, ay, az, pt, ni);
-          dax += ax;
-          day += ay;
-          daz += az;
-          dpot += pt;
+          WALK_STAT(0, nl);
+          evaluate<PERIODIC, POT, TPL>(LP, LH, nl, T, w);
           __syncwarp();
         }
-      if(valid)
+#pragma unroll
+      for(int k = 0; k < TPL; k++)
         {
-          acc_out[3 * t + 0] = dax;
-          acc_out[3 * t + 1] = day;
-          acc_out[3 * t + 2] = daz;
-          if(POT)
-            pot_out[t] = dpot;
-          nint_out[t] = ni;
-          my_total += (unsigned long long)ni;
+          const int64_t t = t0 + lane + 32 * k;
+          if(t < n)
+            {
+              acc_out[3 * t + 0] = T[k].dax;
+              acc_out[3 * t + 1] = T[k].day;
+              acc_out[3 * t + 2] = T[k].daz;
+              if(POT)
+                pot_out[t] = T[k].dpot;
+              nint_out[t] = T[k].ni;
+              my_total += (unsigned long long)T[k].ni;
+            }
         }
     }
   for(int o = 16; o > 0; o >>= 1)
@@ -601,12 +692,16 @@ cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc)
   GG_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const bool periodic = wc.periodic != 0;
   const bool pot      = c->want_pot;
-  auto kern = periodic ? (pot ? k_walk32<true, true> : k_walk32<true, false>) : (pot ? k_walk32<false, true> : k_walk32<false, false>);
+  const int tpl       = (c->walk32_tpl == 1) ? 1 : 2;
+  auto kern = tpl == 2 ? (periodic ? (pot ? k_walk32<true, true, 2> : k_walk32<true, false, 2>)
+                                   : (pot ? k_walk32<false, true, 2> : k_walk32<false, false, 2>))
+                       : (periodic ? (pot ? k_walk32<true, true, 1> : k_walk32<true, false, 1>)
+                                   : (pot ? k_walk32<false, true, 1> : k_walk32<false, false, 1>));
   GG_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * kWarps, 0));
   if(per_sm < 1)
     per_sm = 1;
   const int blocks  = sms * per_sm;
-  const int ngroups = (int)((n + 31) / 32);
+  const int ngroups = (int)((n + 32 * tpl - 1) / (32 * tpl));
   GG_TRY(c->g_stack.ensure((size_t)blocks * kWarps * kStackCap * sizeof(int)));
   int *work = c->counters.as<int>() + 20;
   int *err  = c->counters.as<int>() + 14;
@@ -619,3 +714,14 @@ cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc)
   return cudaGetLastError();
 }
 }  // namespace gg
+
+#ifdef GG_WALK32_STATS
+// measurement build only: read and reset the walk statistics of the current device
+extern "C" int gpugrav_walk_stats(unsigned long long *out)
+{
+  if(cudaMemcpyFromSymbol(out, gg::g_walk_stats, sizeof(unsigned long long) * 4) != cudaSuccess)
+    return -1;
+  unsigned long long z[4] = {0, 0, 0, 0};
+  return cudaMemcpyToSymbol(gg::g_walk_stats, z, sizeof(z)) == cudaSuccess ? 0 : -1;
+}
+#endif
