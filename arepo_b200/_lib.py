@@ -96,6 +96,33 @@ class TreeInfo(C.Structure):
     ]
 
 
+class ServeConfig(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int32),
+        ("max_systems", C.c_int32),
+        ("max_particles", C.c_int64),
+        ("memory_budget_bytes", C.c_int64),
+    ]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_int64),
+        ("admitted", C.c_int64),
+        ("completed", C.c_int64),
+        ("cancelled", C.c_int64),
+        ("waiting", C.c_int64),
+        ("running", C.c_int64),
+        ("in_flight_particles", C.c_int64),
+        ("ticks", C.c_int64),
+        ("particle_steps", C.c_int64),
+        ("last_tick_s", C.c_double),
+        ("last_tick_particles", C.c_int64),
+        ("last_tick_systems", C.c_int32),
+        ("pad", C.c_int32),
+    ]
+
+
 class Timings(C.Structure):
     _fields_ = [
         ("upload_ms", C.c_double),
@@ -136,6 +163,14 @@ _SIGS = {
     "gpugrav_direct": (C.c_int32, [_P, C.c_int64, _P, C.c_int32, _P, _P]),
     "gpugrav_direct_noalloc": (C.c_int32, [C.c_int32, C.POINTER(Params), C.c_int64, _P, _P, _P, C.c_int64, _P, _P,
                                             C.c_int32, _P, _P, _P]),
+    "gpugrav_serve_create": (C.c_int32, [C.POINTER(_P), C.c_int32, C.POINTER(Params), C.POINTER(ServeConfig)]),
+    "gpugrav_serve_destroy": (C.c_int32, [_P]),
+    "gpugrav_serve_last_error": (C.c_char_p, [_P]),
+    "gpugrav_serve_submit": (C.c_int32, [_P, C.c_int64, C.c_int64, _P, _P, _P, _P, C.c_int32, C.c_double]),
+    "gpugrav_serve_cancel": (C.c_int32, [_P, C.c_int64]),
+    "gpugrav_serve_tick": (C.c_int32, [_P, C.POINTER(C.c_int32)]),
+    "gpugrav_serve_poll": (C.c_int32, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), _P, _P, _P, C.c_int64, _P]),
+    "gpugrav_serve_get_stats": (C.c_int32, [_P, C.POINTER(ServeStats)]),
     "gpugrav_measure_fma_peak": (C.c_int32, [C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
 }
 

@@ -29,6 +29,7 @@ SOURCES = [
     ("direct_noalloc.cu", True),
     ("walk32.cu", False),
     ("peak.cu", False),
+    ("serve.cu", False),
     ("gpugrav.cu", True),
 ]
 

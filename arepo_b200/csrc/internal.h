@@ -117,6 +117,11 @@ struct gpugrav_ctx
   gg::DevBuf g_pm, g_pst;                     // particles in parent order: (x, y, z, m) double4; softening type
   gg::DevBuf g_stack;                         // per-warp traversal stacks
   bool layout32_valid = false;
+  // several independent systems in one build (serving): system of each sorted particle, domain of
+  // each system, walk groups (first target, count, root, criterion) that never span two systems
+  bool multi          = false;
+  int32_t m_ngroups   = 0;
+  gg::DevBuf m_sys, m_doms, m_groups;
   bool want_pot       = true;  // potential requested by the current walk call
   int walk32_tpl      = 1;     // targets per lane of the FP32 walk (1 or 2; GPUGRAV_WALK32_TPL)
   gg::DevBuf acc_s, pot_s, nint_s, oldacc_s, oldacc_in;  // per target (sorted), inputs

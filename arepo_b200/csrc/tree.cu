@@ -64,9 +64,14 @@ struct TreeArgs
   const int32_t *tlnode; // top-leaf node (relative index)
   const int32_t *base;   // n+1
   const gpugrav_domain *dom;
+  const int32_t *sys;           // several independent systems: system of each sorted particle (else null)
+  const gpugrav_domain *doms;   // ... and the domain of each system
   int64_t nn;            // node capacity (known after the numbering scan; 0 before)
   int *err;              // self-check flag: set instead of writing out of bounds
 };
+
+// domain whose integer grid particle j lives on
+__device__ __forceinline__ const gpugrav_domain *dom_of(const TreeArgs &a, int64_t j) { return a.sys ? &a.doms[a.sys[j]] : a.dom; }
 
 // node index self-check: every computed node index must lie in [0, nn)
 __device__ __forceinline__ bool node_ok(const TreeArgs &a, int64_t k)
@@ -95,6 +100,8 @@ __device__ __forceinline__ int canon_count(const TreeArgs &a, int64_t j)
 }
 __device__ __forceinline__ int delta(const TreeArgs &a, int64_t p, int64_t q)
 {
+  if(a.sys && a.sys[p] != a.sys[q])
+    return -1;  // different systems share no cell
   return common_depth(a.ix[p], a.iy[p], a.iz[p], a.ix[q], a.iy[q], a.iz[q]);
 }
 // smallest s <= i with delta(s, i) >= d  (start of the depth-d cell containing i)
@@ -499,10 +506,36 @@ __global__ void k_topleaf(const gpugrav_topnode *__restrict__ top, const int32_t
 }
 
 __global__ void k_pairdepth(int64_t n, const uint64_t *__restrict__ ix, const uint64_t *__restrict__ iy,
-                            const uint64_t *__restrict__ iz, int8_t *__restrict__ cd)
+                            const uint64_t *__restrict__ iz, const int32_t *__restrict__ sys, int8_t *__restrict__ cd)
+{
+  // particles of different systems share no cell
+  for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    cd[i] = (i + 1 < n && (!sys || sys[i] == sys[i + 1]))
+                ? (int8_t)common_depth(ix[i], iy[i], iz[i], ix[i + 1], iy[i + 1], iz[i + 1])
+                : (int8_t)-1;
+}
+
+// several systems: node s is the root of system s (len DomainLen, centre DomainCenter of that system)
+__global__ void k_roots(int nsys, const gpugrav_domain *__restrict__ doms, int32_t *__restrict__ suns, double4 *__restrict__ cl,
+                        uint8_t *__restrict__ depth)
+{
+  for(int s = blockIdx.x * blockDim.x + threadIdx.x; s < nsys; s += gridDim.x * blockDim.x)
+    {
+      for(int q = 0; q < 8; q++)
+        suns[8 * (int64_t)s + q] = -1;
+      cl[s]    = make_double4(doms[s].center[0], doms[s].center[1], doms[s].center[2], doms[s].len);
+      depth[s] = 0;
+    }
+}
+
+// several systems: every particle's "top leaf" is its system's root, at depth 0
+__global__ void k_tl_roots(int64_t n, const int32_t *__restrict__ sys, uint8_t *__restrict__ tl, int32_t *__restrict__ tlnode)
 {
   for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    cd[i] = (i + 1 < n) ? (int8_t)common_depth(ix[i], iy[i], iz[i], ix[i + 1], iy[i + 1], iz[i + 1]) : (int8_t)-1;
+    {
+      tl[i]     = 0;
+      tlnode[i] = sys[i];
+    }
 }
 
 // canonical node count per inserting particle + detection of replayed (coincident) cells
@@ -656,11 +689,12 @@ __device__ void replay_cell(const TreeArgs &a, const HackCell &c, int32_t *suns,
               SUN(parent, subnode) = (int32_t)(nf + n);
               if(FILL)
                 {
-                  const double bf = a.dom->big_fac;
-                  double len      = __dmul_rn((double)(mask << 1), bf);
-                  double cx = __dadd_rn(__dmul_rn((double)((xxb & (uint64_t)centermask) | mask), bf), a.dom->corner[0]);
-                  double cy = __dadd_rn(__dmul_rn((double)((yyb & (uint64_t)centermask) | mask), bf), a.dom->corner[1]);
-                  double cz = __dadd_rn(__dmul_rn((double)((zzb & (uint64_t)centermask) | mask), bf), a.dom->corner[2]);
+                  const gpugrav_domain *dm = dom_of(a, q);
+                  const double bf          = dm->big_fac;
+                  double len               = __dmul_rn((double)(mask << 1), bf);
+                  double cx = __dadd_rn(__dmul_rn((double)((xxb & (uint64_t)centermask) | mask), bf), dm->corner[0]);
+                  double cy = __dadd_rn(__dmul_rn((double)((yyb & (uint64_t)centermask) | mask), bf), dm->corner[1]);
+                  double cz = __dadd_rn(__dmul_rn((double)((zzb & (uint64_t)centermask) | mask), bf), dm->corner[2]);
                   cl[nf]     = make_double4(cx, cy, cz, len);
                   depth[nf]  = (uint8_t)(levels > 255 ? 255 : levels);
                   father[nf] = (int32_t)parent;
@@ -709,7 +743,8 @@ __global__ void k_nodes(TreeArgs a, int32_t *__restrict__ suns, double4 *__restr
       int d0          = dstart_of(a, j);
       int64_t k0      = (int64_t)a.ntop + a.base[j];
       uint64_t x = a.ix[j], y = a.iy[j], z = a.iz[j];
-      const double bf = a.dom->big_fac;
+      const gpugrav_domain *dm = dom_of(a, j);
+      const double bf          = dm->big_fac;
       for(int t = 0; t < cnt; t++)
         {
           int d      = d0 + t;
@@ -717,9 +752,9 @@ __global__ void k_nodes(TreeArgs a, int32_t *__restrict__ suns, double4 *__restr
           uint64_t m = 1ull << (51 - d);
           uint64_t keep = ~((1ull << (52 - d)) - 1ull);
           double len = __dmul_rn((double)(m << 1), bf);
-          double cx  = __dadd_rn(__dmul_rn((double)((x & keep) | m), bf), a.dom->corner[0]);
-          double cy  = __dadd_rn(__dmul_rn((double)((y & keep) | m), bf), a.dom->corner[1]);
-          double cz  = __dadd_rn(__dmul_rn((double)((z & keep) | m), bf), a.dom->corner[2]);
+          double cx  = __dadd_rn(__dmul_rn((double)((x & keep) | m), bf), dm->corner[0]);
+          double cy  = __dadd_rn(__dmul_rn((double)((y & keep) | m), bf), dm->corner[1]);
+          double cz  = __dadd_rn(__dmul_rn((double)((z & keep) | m), bf), dm->corner[2]);
           cl[k]      = make_double4(cx, cy, cz, len);
           depth[k]   = (uint8_t)d;
           first[k]   = (int32_t)(j - 1);
@@ -910,6 +945,16 @@ __global__ void k_dfs(const int32_t *__restrict__ order, int count, int64_t n, c
   nnext[k] = (m > 0) ? c[0] : SIB;
 }
 
+// several systems: traversal positions of the roots (exclusive prefix of their subtree sizes, in ndfs)
+__global__ void k_roots_finish(int nsys, int32_t *nsib, int32_t *nfather)
+{
+  for(int s = blockIdx.x * blockDim.x + threadIdx.x; s < nsys; s += gridDim.x * blockDim.x)
+    {
+      nsib[s]    = -1;
+      nfather[s] = -1;
+    }
+}
+
 __global__ void k_root_init(int32_t *ndfs, int32_t *nsib, int32_t *nfather)
 {
   ndfs[0]    = 0;
@@ -1067,26 +1112,40 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
   };
 
   // 1. per-particle top leaf, pair depths (skeleton first: it validates the top tree and maps leaves to nodes)
+  const int32_t *msys            = c->multi ? c->m_sys.as<int32_t>() : nullptr;
+  const gpugrav_domain *mdoms    = c->multi ? c->m_doms.as<gpugrav_domain>() : nullptr;
   GG_TRY(ensure_nodes(ntop + 16));
-  k_skeleton<<<1, 32, 0, st>>>(c->top.as<gpugrav_topnode>(), ntop, c->bconst.as<BuildConst>(), c->n_suns.as<int32_t>(),
-                                c->n_cl.as<double4>(), c->n_depth.as<uint8_t>(), leafnode, nodetop, sinfo);
-  launches++;
-  SkelInfo si;
-  GG_TRY(cudaMemcpyAsync(&si, sinfo, sizeof(si), cudaMemcpyDeviceToHost, st));
-  GG_TRY(cudaStreamSynchronize(st));
-  if(si.status < 0 || si.ntop_nodes != ntop)
+  if(c->multi)
     {
-      *status = GPUGRAV_ERR_TOPNODES;
-      return cudaSuccess;
+      // independent systems: one root per system, no top-level skeleton below it
+      k_roots<<<grid_for(ntop, 128), 128, 0, st>>>(ntop, mdoms, c->n_suns.as<int32_t>(), c->n_cl.as<double4>(),
+                                                    c->n_depth.as<uint8_t>());
+      k_tl_roots<<<grid_for(n, 256), 256, 0, st>>>(n, msys, c->s_tl.as<uint8_t>(), c->s_tlnode.as<int32_t>());
+      c->nleaves = ntop;
+      launches += 2;
     }
-  c->nleaves = si.nleaves;
-
-  k_topleaf<<<grid_for(n, 256), 256, 0, st>>>(c->top.as<gpugrav_topnode>(), leafnode, n, c->s_ix.as<uint64_t>(),
-                                               c->s_iy.as<uint64_t>(), c->s_iz.as<uint64_t>(), c->s_tl.as<uint8_t>(),
-                                               c->s_tlnode.as<int32_t>());
-  k_pairdepth<<<grid_for(n, 256), 256, 0, st>>>(n, c->s_ix.as<uint64_t>(), c->s_iy.as<uint64_t>(), c->s_iz.as<uint64_t>(),
+  else
+    {
+      k_skeleton<<<1, 32, 0, st>>>(c->top.as<gpugrav_topnode>(), ntop, c->bconst.as<BuildConst>(), c->n_suns.as<int32_t>(),
+                                    c->n_cl.as<double4>(), c->n_depth.as<uint8_t>(), leafnode, nodetop, sinfo);
+      launches++;
+      SkelInfo si;
+      GG_TRY(cudaMemcpyAsync(&si, sinfo, sizeof(si), cudaMemcpyDeviceToHost, st));
+      GG_TRY(cudaStreamSynchronize(st));
+      if(si.status < 0 || si.ntop_nodes != ntop)
+        {
+          *status = GPUGRAV_ERR_TOPNODES;
+          return cudaSuccess;
+        }
+      c->nleaves = si.nleaves;
+      k_topleaf<<<grid_for(n, 256), 256, 0, st>>>(c->top.as<gpugrav_topnode>(), leafnode, n, c->s_ix.as<uint64_t>(),
+                                                   c->s_iy.as<uint64_t>(), c->s_iz.as<uint64_t>(), c->s_tl.as<uint8_t>(),
+                                                   c->s_tlnode.as<int32_t>());
+      launches++;
+    }
+  k_pairdepth<<<grid_for(n, 256), 256, 0, st>>>(n, c->s_ix.as<uint64_t>(), c->s_iy.as<uint64_t>(), c->s_iz.as<uint64_t>(), msys,
                                                  c->s_cd.as<int8_t>());
-  launches += 2;
+  launches++;
 
   TreeArgs a;
   a.n      = n;
@@ -1101,6 +1160,8 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
   a.tlnode = c->s_tlnode.as<int32_t>();
   a.base   = c->base.as<int32_t>();
   a.dom    = &c->bconst.as<BuildConst>()->dom;
+  a.sys    = msys;
+  a.doms   = mdoms;
   a.nn     = 0;
   a.err    = counters + 12;
 
@@ -1166,8 +1227,12 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
       for(auto *b : bufs)
         b->release();
       GG_TRY(ensure_nodes(nn + 16));
-      k_skeleton<<<1, 32, 0, st>>>(c->top.as<gpugrav_topnode>(), ntop, c->bconst.as<BuildConst>(), c->n_suns.as<int32_t>(),
-                                    c->n_cl.as<double4>(), c->n_depth.as<uint8_t>(), leafnode, nodetop, sinfo);
+      if(c->multi)
+        k_roots<<<grid_for(ntop, 128), 128, 0, st>>>(ntop, mdoms, c->n_suns.as<int32_t>(), c->n_cl.as<double4>(),
+                                                      c->n_depth.as<uint8_t>());
+      else
+        k_skeleton<<<1, 32, 0, st>>>(c->top.as<gpugrav_topnode>(), ntop, c->bconst.as<BuildConst>(), c->n_suns.as<int32_t>(),
+                                      c->n_cl.as<double4>(), c->n_depth.as<uint8_t>(), leafnode, nodetop, sinfo);
       launches++;
     }
 
@@ -1226,7 +1291,17 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
   GG_TRY(c->p_next.ensure((n + 16) * sizeof(int32_t)));
   GG_TRY(c->p_father.ensure((n + 16) * sizeof(int32_t)));
   GG_TRY(c->p_dfs.ensure((n + 16) * sizeof(int32_t)));
-  k_root_init<<<1, 1, 0, st>>>(c->n_dfs.as<int32_t>(), c->n_sibling.as<int32_t>(), c->n_father.as<int32_t>());
+  if(c->multi)
+    {
+      // each system's traversal follows the previous one's: roots at the prefix sums of the subtree sizes
+      size_t tb = 0;
+      GG_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, c->n_size.as<int32_t>(), c->n_dfs.as<int32_t>(), ntop, st));
+      GG_TRY(c->sort_tmp.ensure(tb));
+      GG_TRY(cub::DeviceScan::ExclusiveSum(c->sort_tmp.p, tb, c->n_size.as<int32_t>(), c->n_dfs.as<int32_t>(), ntop, st));
+      k_roots_finish<<<grid_for(ntop, 128), 128, 0, st>>>(ntop, c->n_sibling.as<int32_t>(), c->n_father.as<int32_t>());
+    }
+  else
+    k_root_init<<<1, 1, 0, st>>>(c->n_dfs.as<int32_t>(), c->n_sibling.as<int32_t>(), c->n_father.as<int32_t>());
   launches++;
   for(int d = 0; d <= maxd; d++)
     {

@@ -338,7 +338,8 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                                                         const int4 *__restrict__ g_kids, const double4 *__restrict__ g_pm,
                                                         const uint8_t *__restrict__ g_pst, const double4 *__restrict__ tpm,
                                                         const uint8_t *__restrict__ tst, const float *__restrict__ oldacc,
-                                                        int64_t n, int ngroups, const W32Const *__restrict__ wcp,
+                                                        int64_t n, int ngroups, const int4 *__restrict__ groups,
+                                                        const W32Const *__restrict__ wcp,
                                                         int *__restrict__ stack_base, int *__restrict__ work,
                                                         double *__restrict__ acc_out, double *__restrict__ pot_out,
                                                         int32_t *__restrict__ nint_out, unsigned long long *__restrict__ total,
@@ -368,8 +369,23 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
       if(grp >= ngroups)
         break;
       WALK_STAT(3, 1);
-      // group of 32*TPL consecutive targets; lane holds targets t0 + lane + 32k
-      const int64_t t0 = (int64_t)grp * 32 * TPL;
+      // group of up to 32*TPL consecutive targets; lane holds targets t0 + lane + 32k.  With a group
+      // table (several systems) a group lies inside one system and walks that system's tree.
+      int64_t t0, tend;
+      int root = 0, bh = w.bh;
+      if(groups)
+        {
+          const int4 G = groups[grp];
+          t0           = G.x;
+          tend         = (int64_t)G.x + G.y;
+          root         = G.z;
+          bh           = G.w;
+        }
+      else
+        {
+          t0   = (int64_t)grp * 32 * TPL;
+          tend = t0 + 32 * TPL < n ? t0 + 32 * TPL : n;
+        }
       double4 p[TPL];
       double mnx = 1e300, mxx = -1e300, mny = 1e300, mxy = -1e300, mnz = 1e300, mxz = -1e300;
       float hmin_l = 3.0e38f, amin_l = 3.0e38f;
@@ -377,7 +393,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
       for(int k = 0; k < TPL; k++)
         {
           const int64_t t  = t0 + lane + 32 * k;
-          const int64_t tt = t < n ? t : t0;  // idle slots repeat the group's first target
+          const int64_t tt = t < tend ? t : t0;  // idle slots repeat the group's first target
           p[k]             = tpm[tt];
           mnx = fmin(mnx, p[k].x), mxx = fmax(mxx, p[k].x);
           mny = fmin(mny, p[k].y), mxy = fmax(mxy, p[k].y);
@@ -397,7 +413,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
       for(int k = 0; k < TPL; k++)
         {
           const int64_t t  = t0 + lane + 32 * k;
-          const int64_t tt = t < n ? t : t0;
+          const int64_t tt = t < tend ? t : t0;
           T[k].x = (float)(p[k].x - gx), T[k].y = (float)(p[k].y - gy), T[k].z = (float)(p[k].z - gz);
           T[k].h  = w.soft[tst[tt]];
           T[k].ax = T[k].ay = T[k].az = T[k].pot = 0.0f;
@@ -407,7 +423,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
 
       int nl = 0, sp = 1;
       if(lane == 0)
-        stack[0] = 0;  // root
+        stack[0] = root;
       __syncwarp();
 
       while(sp > 0)
@@ -449,7 +465,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                       const float rmin2 = dmx * dmx + dmy * dmy + dmz * dmz;
                       const float L2    = L * L;
                       bool open;
-                      if(w.bh)
+                      if(bh)
                         open = L2 > rmin2 * w.theta2;
                       else
                         open = (L2 > rmin2 * 1.44f) || (m * L2 > rmin2 * rmin2 * aold_min) ||
@@ -568,7 +584,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
       for(int k = 0; k < TPL; k++)
         {
           const int64_t t = t0 + lane + 32 * k;
-          if(t < n)
+          if(t < tend)
             {
               acc_out[3 * t + 0] = T[k].dax;
               acc_out[3 * t + 1] = T[k].day;
@@ -692,7 +708,7 @@ cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc)
   GG_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const bool periodic = wc.periodic != 0;
   const bool pot      = c->want_pot;
-  const int tpl       = (c->walk32_tpl == 1) ? 1 : 2;
+  const int tpl       = (c->walk32_tpl == 1 || c->multi) ? 1 : 2;
   auto kern = tpl == 2 ? (periodic ? (pot ? k_walk32<true, true, 2> : k_walk32<true, false, 2>)
                                    : (pot ? k_walk32<false, true, 2> : k_walk32<false, false, 2>))
                        : (periodic ? (pot ? k_walk32<true, true, 1> : k_walk32<true, false, 1>)
@@ -701,14 +717,15 @@ cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc)
   if(per_sm < 1)
     per_sm = 1;
   const int blocks  = sms * per_sm;
-  const int ngroups = (int)((n + 32 * tpl - 1) / (32 * tpl));
+  const int ngroups = c->multi ? c->m_ngroups : (int)((n + 32 * tpl - 1) / (32 * tpl));
   GG_TRY(c->g_stack.ensure((size_t)blocks * kWarps * kStackCap * sizeof(int)));
   int *work = c->counters.as<int>() + 20;
   int *err  = c->counters.as<int>() + 14;
   GG_TRY(cudaMemsetAsync(work, 0, sizeof(int), st));
   kern<<<blocks, 32 * kWarps, 0, st>>>(c->g_sm.as<double4>(), c->g_rel.as<float4>(), c->g_kids.as<int4>(), c->g_pm.as<double4>(),
                                        c->g_pst.as<uint8_t>(), c->s_pm.as<double4>(), c->s_st.as<uint8_t>(),
-                                       c->oldacc_s.as<float>(), n, ngroups, (const W32Const *)c->scratch.p, c->g_stack.as<int>(),
+                                       c->oldacc_s.as<float>(), n, ngroups, c->multi ? c->m_groups.as<int4>() : nullptr,
+                                       (const W32Const *)c->scratch.p, c->g_stack.as<int>(),
                                        work, c->acc_s.as<double>(), c->pot_s.as<double>(), c->nint_s.as<int32_t>(),
                                        (unsigned long long *)(c->counters.as<int>() + 32), err);
   return cudaGetLastError();

@@ -209,6 +209,53 @@ enum
 };
 int32_t gpugrav_direct(gpugrav_ctx *ctx, int64_t ntargets, const int64_t *targets, int32_t mode, double *acc, double *pot);
 
+/* ---- serving loop: many independent isolated systems, continuously batched ----
+ * Each submitted request is one isolated N-body system (G = 1 units of the params' softening table)
+ * that runs what the reference runs on its first step and afterwards: a Barnes-Hut force pass
+ * (err_tol_theta), a relative-criterion pass (err_tol_force_acc), then nsteps kick-drift-kick
+ * leapfrog steps of size dt (kick_particle, src/time_integration/do_gravity_hydro.c:63-83;
+ * drift_particle, src/time_integration/predict.c:357-425), with the FP32 walk.
+ * Requests are admitted at tick boundaries in arrival order while system slots, the particle pool
+ * and the device-memory budget allow; gpugrav_serve_tick advances every admitted system by one
+ * force evaluation in one batched build and one persistent walk. Results stay on the host until
+ * polled. No counterpart in the reference (it integrates one system per run). */
+typedef struct gpugrav_serve gpugrav_serve;
+
+typedef struct gpugrav_serve_config
+{
+  int32_t abi_version;          /* GPUGRAV_ABI_VERSION */
+  int32_t max_systems;          /* systems in flight at once (1 = one request at a time) */
+  int64_t max_particles;        /* particle pool: particles in flight at once */
+  int64_t memory_budget_bytes;  /* admission budget for the device footprint of the particles in flight (0: pool only) */
+} gpugrav_serve_config;
+
+typedef struct gpugrav_serve_stats
+{
+  int64_t submitted, admitted, completed, cancelled;
+  int64_t waiting, running, in_flight_particles;
+  int64_t ticks, particle_steps;  /* force evaluations x particles, summed over ticks */
+  double last_tick_s;
+  int64_t last_tick_particles;
+  int32_t last_tick_systems;
+  int32_t pad;
+} gpugrav_serve_stats;
+
+int32_t gpugrav_serve_create(gpugrav_serve **srv, int32_t device, const gpugrav_params *params,
+                             const gpugrav_serve_config *cfg);
+int32_t gpugrav_serve_destroy(gpugrav_serve *srv);
+const char *gpugrav_serve_last_error(gpugrav_serve *srv);
+/* host arrays, copied: pos, vel n*3; mass n; softtype n */
+int32_t gpugrav_serve_submit(gpugrav_serve *srv, int64_t id, int64_t n, const double *pos, const double *vel,
+                             const double *mass, const uint8_t *softtype, int32_t nsteps, double dt);
+int32_t gpugrav_serve_cancel(gpugrav_serve *srv, int64_t id);
+/* one force evaluation for every admitted system (admission first); n_active may be NULL */
+int32_t gpugrav_serve_tick(gpugrav_serve *srv, int32_t *n_active);
+/* oldest finished request: *id = -1 when none. With capacity < *n only id and n are returned and the
+ * result stays queued. times (may be NULL): submit, admit, done (seconds, steady clock). */
+int32_t gpugrav_serve_poll(gpugrav_serve *srv, int64_t *id, int64_t *n, double *pos, double *vel, double *acc,
+                           int64_t capacity, double *times);
+int32_t gpugrav_serve_get_stats(gpugrav_serve *srv, gpugrav_serve_stats *stats);
+
 /* ---- direct summation without allocation (no counterpart in the reference) ----
  * The same FP64 sum as gpugrav_direct, for callers that cannot allocate device memory at the point
  * of the call (their device memory belongs to their own pool allocator, or they cannot accept the

@@ -1,0 +1,131 @@
+"""Serving loop (gpugrav_serve_*): each request's result is the same alone and in
+a mix of other requests at other stages, forces agree with FP64 direct summation,
+the kick-drift-kick sequence matches a numpy leapfrog on the same forces, and
+admission, cancellation and errors behave."""
+import numpy as np
+import pytest
+
+from arepo_b200 import _lib as L
+from arepo_b200 import ics
+from arepo_b200.gravity import GravityTree
+from arepo_b200.serving import GravityServer, serving_params
+
+pytestmark = pytest.mark.gpu
+
+EPS = 0.02
+
+
+def _system(kind, n, seed):
+    ic = ics.plummer(n, seed) if kind == "plummer" else ics.hernquist(n, seed=seed, eps=EPS)
+    vel = np.zeros_like(ic["pos"])
+    return ic["pos"], vel, ic["mass"], ic["softtype"]
+
+
+def test_alone_equals_in_the_mix(cuda_lib):
+    prm = serving_params(EPS)
+    target = _system("plummer", 3000, 7)
+    with GravityServer(prm, max_systems=1, max_particles=1 << 20) as srv:
+        srv.submit(1, *target, nsteps=5, dt=0.005)
+        alone = srv.run_to_completion()[1]
+    with GravityServer(prm, max_systems=64, max_particles=1 << 21) as srv:
+        # others arrive before, with, and after the target, with different sizes and step counts
+        srv.submit(10, *_system("hernquist", 20000, 11), nsteps=3, dt=0.005)
+        srv.tick()
+        srv.submit(11, *_system("plummer", 1500, 12), nsteps=9, dt=0.01)
+        srv.submit(1, *target, nsteps=5, dt=0.005)
+        srv.tick()
+        srv.submit(12, *_system("hernquist", 70000, 13), nsteps=2, dt=0.005)
+        res = srv.run_to_completion()
+    mix = res[1]
+    assert set(res) == {1, 10, 11, 12}
+    assert np.array_equal(mix.pos, alone.pos)
+    assert np.array_equal(mix.vel, alone.vel)
+    assert np.array_equal(mix.acc, alone.acc)
+
+
+@pytest.mark.parametrize("kind", ["plummer", "hernquist"])
+def test_served_force_matches_direct_sum(kind, cuda_lib):
+    pos, vel, mass, st = _system(kind, 20000, 21)
+    prm = serving_params(EPS)
+    with GravityServer(prm, max_systems=4, max_particles=1 << 20) as srv:
+        srv.submit(5, pos, vel, mass, st, nsteps=0, dt=0.0)
+        r = srv.run_to_completion()[5]
+    assert np.array_equal(r.pos, pos)
+    with GravityTree(L.make_params(periodic=False, softening=(EPS,))) as t:
+        t.domain_decomposition(pos, mass, st)
+        tg = np.arange(0, len(mass), 5)
+        d, _ = t.direct(tg)
+    e = np.linalg.norm(r.acc[tg] - d, axis=1) / np.linalg.norm(d, axis=1)
+    assert np.sqrt(np.mean(e ** 2)) < 5e-3  # relative criterion at ErrTolForceAcc = 0.0025
+    assert np.percentile(e, 99) < 2e-2
+
+
+def test_kick_drift_kick_matches_numpy_leapfrog(cuda_lib):
+    """Same KDK sequence in numpy with the served force replaced by FP64 direct summation: the
+    trajectories differ only by the tree's force error over a few steps."""
+    pos, vel, mass, st = _system("plummer", 2000, 31)
+    rng = np.random.default_rng(3)
+    vel = 0.3 * rng.normal(size=pos.shape)
+    dt, k = 0.01, 4
+    prm = serving_params(EPS, err_tol_force_acc=1e-5)  # tight criterion: close to the direct sum
+    with GravityServer(prm, max_systems=2, max_particles=1 << 16) as srv:
+        srv.submit(3, pos, vel, mass, st, nsteps=k, dt=dt)
+        r = srv.run_to_completion()[3]
+
+    def direct(x):
+        with GravityTree(L.make_params(periodic=False, softening=(EPS,))) as t:
+            t.domain_decomposition(x, mass, st)
+            a, _ = t.direct(np.arange(len(mass)))
+        return a
+
+    x, v = pos.copy(), vel.copy()
+    a = direct(x)
+    for _ in range(k):
+        v = v + 0.5 * dt * a
+        x = x + dt * v
+        a = direct(x)
+        v = v + 0.5 * dt * a
+    scale = np.sqrt(np.mean(np.sum(a * a, axis=1)))
+    assert np.max(np.abs(r.pos - x)) < 1e-6 * (1 + np.max(np.abs(x)))
+    assert np.sqrt(np.mean(np.sum((r.acc - a) ** 2, axis=1))) < 1e-3 * scale
+    assert np.max(np.abs(r.vel - v)) < 1e-4 * (np.max(np.abs(v)) + 1)
+
+
+def test_admission_by_budget_and_cancel(cuda_lib):
+    prm = serving_params(EPS)
+    a = _system("plummer", 4000, 41)
+    b = _system("plummer", 4000, 42)
+    c = _system("plummer", 4000, 43)
+    # budget for ~1.5 systems of 4000 particles: the second waits until the first finishes
+    with GravityServer(prm, max_systems=16, max_particles=1 << 16, budget_bytes=6000 * 700) as srv:
+        srv.submit(1, *a, nsteps=2, dt=0.005)
+        srv.submit(2, *b, nsteps=2, dt=0.005)
+        srv.submit(3, *c, nsteps=2, dt=0.005)
+        srv.tick()
+        st = srv.stats()
+        assert st.running == 1 and st.waiting == 2
+        srv.cancel(3)
+        res = srv.run_to_completion()
+        st = srv.stats()
+        assert set(res) == {1, 2} and st.cancelled == 1 and st.completed == 2
+        assert res[2].t_admit >= res[1].t_done - 1e-3
+        with pytest.raises(L.GpuGravError):
+            srv.cancel(99)
+
+
+def test_submit_errors(cuda_lib):
+    prm = serving_params(EPS)
+    pos, vel, mass, st = _system("plummer", 1000, 51)
+    with GravityServer(prm, max_systems=2, max_particles=4096) as srv:
+        bad = pos.copy()
+        bad[3, 0] = np.inf
+        with pytest.raises(L.GpuGravError):
+            srv.submit(1, bad, vel, mass, st, nsteps=1, dt=0.01)
+        with pytest.raises(L.GpuGravError) as e:
+            big = _system("plummer", 5000, 52)
+            srv.submit(2, *big, nsteps=1, dt=0.01)
+        assert e.value.status == L.ERR_TOO_LARGE
+        st2 = st.copy()
+        st2[0] = 3
+        with pytest.raises(L.GpuGravError):
+            srv.submit(3, pos, vel, mass, st2, nsteps=1, dt=0.01)
