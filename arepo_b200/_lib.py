@@ -120,6 +120,13 @@ class ServeStats(C.Structure):
         ("last_tick_particles", C.c_int64),
         ("last_tick_systems", C.c_int32),
         ("pad", C.c_int32),
+        ("graph_captures", C.c_int64),
+        ("graph_replays", C.c_int64),
+        ("admit_s", C.c_double),
+        ("build_s", C.c_double),
+        ("walk_s", C.c_double),
+        ("finish_s", C.c_double),
+        ("interactions", C.c_int64),
     ]
 
 

@@ -277,6 +277,8 @@ int32_t gpugrav_create(gpugrav_ctx **out, int32_t device, const gpugrav_params *
   c->prm    = *p;
   if(const char *e = getenv("GPUGRAV_WALK32_TPL"))
     c->walk32_tpl = atoi(e) == 1 ? 1 : 2;
+  if(const char *e = getenv("GPUGRAV_GROUP_SLACK"))
+    c->group_slack = atoi(e);
   DeviceGuard g(device);
   if(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     {
@@ -312,7 +314,8 @@ int32_t gpugrav_destroy(gpugrav_ctx *c)
                         &c->n_suns, &c->n_depth, &c->n_cl, &c->n_sm, &c->n_maxsoft, &c->n_size, &c->n_father, &c->n_sibling,
                         &c->n_next, &c->n_dfs, &c->n_first, &c->p_next, &c->p_father, &c->p_dfs, &c->depth_hist,
                         &c->depth_order, &c->w_sm, &c->w_cl, &c->w_link, &c->g_key, &c->g_key_alt, &c->g_val, &c->g_val_alt, &c->g_bfs, &c->g_np, &c->g_poff, &c->g_sm, &c->g_rel, &c->g_kids, &c->g_pm, &c->g_pst, &c->g_stack, &c->acc_s, &c->pot_s,
-                        &c->nint_s, &c->oldacc_s, &c->oldacc_in, &c->out_acc, &c->out_pot, &c->out_nint, &c->scratch};
+                        &c->nint_s, &c->oldacc_s, &c->oldacc_in, &c->out_acc, &c->out_pot, &c->out_nint, &c->scratch,
+                        &c->g_groups, &c->g_ngroups, &c->g_gpd, &c->g_gseg, &c->g_gflag, &c->g_gid, &c->m_sys, &c->m_doms};
   for(auto *b : bufs)
     b->release();
   c->pinned.release();

@@ -116,12 +116,17 @@ struct gpugrav_ctx
   gg::DevBuf g_sm, g_rel, g_kids;             // node: (CoM, mass) double4; (centre - CoM, len) float4; int4 links
   gg::DevBuf g_pm, g_pst;                     // particles in parent order: (x, y, z, m) double4; softening type
   gg::DevBuf g_stack;                         // per-warp traversal stacks
+  gg::DevBuf g_groups, g_ngroups;             // walk groups (first, count, root, criterion), their count
+  gg::DevBuf g_gpd, g_gseg, g_gflag, g_gid;   // group construction scratch
+  int group_slack = 99;                       // group cuts between cells (< 64) or key order only (GPUGRAV_GROUP_SLACK)
   bool layout32_valid = false;
   // several independent systems in one build (serving): system of each sorted particle, domain of
-  // each system, walk groups (first target, count, root, criterion) that never span two systems
-  bool multi          = false;
-  int32_t m_ngroups   = 0;
-  gg::DevBuf m_sys, m_doms, m_groups;
+  // each system (walk groups never span two systems)
+  bool multi = false;
+  gg::DevBuf m_sys, m_doms;
+  // FP32 walk launch plan (walk32_prepare)
+  void *w32_kernel   = nullptr;
+  int32_t w32_blocks = 0;
   bool want_pot       = true;  // potential requested by the current walk call
   int walk32_tpl      = 1;     // targets per lane of the FP32 walk (1 or 2; GPUGRAV_WALK32_TPL)
   gg::DevBuf acc_s, pot_s, nint_s, oldacc_s, oldacc_in;  // per target (sorted), inputs
@@ -144,6 +149,9 @@ cudaError_t skeleton_stage(gpugrav_ctx *c, int *status);
 cudaError_t build_stage(gpugrav_ctx *c, int *status);
 cudaError_t walk64_stage(gpugrav_ctx *c, const WalkConst &wc);
 cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc);
+cudaError_t walk32_prepare(gpugrav_ctx *c, const WalkConst &wc);
+cudaError_t walk32_launch(gpugrav_ctx *c);
+cudaError_t groups_stage(gpugrav_ctx *c);
 cudaError_t layout32_stage(gpugrav_ctx *c);
 cudaError_t direct_stage(gpugrav_ctx *c, const WalkConst &wc, int64_t nt, const int64_t *d_targets, int cut, double *d_acc,
                          double *d_pot);

@@ -44,7 +44,6 @@ struct SysDev
 {
   int64_t pool_off;  // first particle in the pool
   int64_t coff;      // first particle in tick-compact (and sorted) order
-  int64_t goff;      // first walk group
   int32_t n;
   int32_t state;
   double dt;
@@ -202,18 +201,12 @@ __global__ void k_srv_gather(int64_t ntot, const uint32_t *__restrict__ sorted_i
     }
 }
 
-// walk groups: 32 consecutive targets of one system, root = the system's root, criterion per state
-__global__ void k_srv_groups(int ngroups, int nsys, const SysDev *__restrict__ sys, const int64_t *__restrict__ gstart,
-                             int4 *__restrict__ groups)
+// criterion per group: Barnes-Hut for systems on their first force evaluation
+__global__ void k_srv_bh(const int *__restrict__ ngroups, const SysDev *__restrict__ sys, int4 *__restrict__ groups)
 {
-  for(int g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gridDim.x * blockDim.x)
-    {
-      int s           = find_sys(gstart, nsys, g);
-      int64_t k       = g - sys[s].goff;
-      int64_t first   = sys[s].coff + 32 * k;
-      int64_t remain  = sys[s].n - 32 * k;
-      groups[g] = make_int4((int)first, (int)(remain < 32 ? remain : 32), s, sys[s].state == ST_NEW ? 1 : 0);
-    }
+  const int ng = *ngroups;
+  for(int g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x)
+    groups[g].w = sys[groups[g].z].state == ST_NEW ? 1 : 0;
 }
 
 // store forces, kick the stepping systems, OldAcc = |a| for the next relative pass
@@ -289,13 +282,13 @@ struct gpugrav_serve
   int64_t bytes_per_particle = 0;
 
   gg::DevBuf pos, vel, acc, oldacc, stype;  // particle pool
-  gg::DevBuf sysdev, cstart, gstart, c2p, csys, s2p, ntot_dev;
+  gg::DevBuf sysdev, cstart, c2p, csys, s2p, ntot_dev;
   gg::PinnedBuf staging;
 
-  // captured walk + post-processing graph
+  // captured walk + store/kick graph; re-captured when a buffer it names moves
   cudaGraphExec_t graph = nullptr;
-  std::vector<void *> graph_ptrs;
-  int64_t graph_ntot = -1;
+  std::vector<const void *> graph_key;
+  int64_t graph_captures = 0, graph_replays = 0;
 
   gpugrav_serve_stats stats{};
   std::string err;
@@ -409,7 +402,6 @@ int32_t gpugrav_serve_create(gpugrav_serve **out, int32_t device, const gpugrav_
             s->stype.ensure(s->pool_cap + 16) == cudaSuccess &&
             s->sysdev.ensure((size_t)cfg->max_systems * sizeof(SysDev)) == cudaSuccess &&
             s->cstart.ensure((size_t)(cfg->max_systems + 1) * 8) == cudaSuccess &&
-            s->gstart.ensure((size_t)(cfg->max_systems + 1) * 8) == cudaSuccess &&
             s->c2p.ensure(s->pool_cap * 8) == cudaSuccess && s->csys.ensure(s->pool_cap * 4) == cudaSuccess &&
             s->s2p.ensure(s->pool_cap * 8) == cudaSuccess && s->ntot_dev.ensure(64) == cudaSuccess;
   // the build context's constants (isolated, softening table)
@@ -451,7 +443,7 @@ int32_t gpugrav_serve_destroy(gpugrav_serve *s)
   for(auto *r : s->finished)
     delete r;
   gg::DevBuf *bufs[] = {&s->pos, &s->vel, &s->acc, &s->oldacc, &s->stype, &s->sysdev, &s->cstart,
-                        &s->gstart, &s->c2p, &s->csys, &s->s2p, &s->ntot_dev};
+                        &s->c2p, &s->csys, &s->s2p, &s->ntot_dev};
   for(auto *b : bufs)
     b->release();
   s->staging.release();
@@ -467,7 +459,7 @@ const char *gpugrav_serve_last_error(gpugrav_serve *s) { return s ? s->err.c_str
 int32_t gpugrav_serve_submit(gpugrav_serve *s, int64_t id, int64_t n, const double *pos, const double *vel, const double *mass,
                              const uint8_t *softtype, int32_t nsteps, double dt)
 {
-  if(!s || n < 2 || !pos || !vel || !mass || !softtype || nsteps < 0 || !(dt >= 0) || !std::isfinite(dt))
+  if(!s || id < 0 || n < 2 || !pos || !vel || !mass || !softtype || nsteps < 0 || !(dt >= 0) || !std::isfinite(dt))
     return GPUGRAV_ERR_INVALID;
   if(n > s->pool_cap || n > (int64_t)1 << 30)
     return sfail(s, GPUGRAV_ERR_TOO_LARGE, "request larger than the particle pool");
@@ -566,6 +558,8 @@ int32_t gpugrav_serve_tick(gpugrav_serve *s, int32_t *n_active)
       s->active.push_back(r);
       s->stats.admitted++;
     }
+  const double t_admitted = now_s();
+  s->stats.admit_s += t_admitted - t_tick;
   const int nsys = (int)s->active.size();
   if(n_active)
     *n_active = nsys;
@@ -574,29 +568,26 @@ int32_t gpugrav_serve_tick(gpugrav_serve *s, int32_t *n_active)
 
   // ---- system table ----
   std::vector<SysDev> sd(nsys);
-  std::vector<int64_t> cst(nsys), gst(nsys);
-  int64_t ntot = 0, ng = 0;
+  std::vector<int64_t> cst(nsys);
+  int64_t ntot = 0;
   for(int k = 0; k < nsys; k++)
     {
       auto *r       = s->active[k];
       sd[k].pool_off = r->pool_off;
       sd[k].coff     = ntot;
-      sd[k].goff     = ng;
       sd[k].n        = (int32_t)r->n;
       sd[k].state    = r->state;
       sd[k].dt       = r->dt;
       cst[k]         = ntot;
-      gst[k]         = ng;
       ntot += r->n;
-      ng += (r->n + 31) / 32;
     }
   SCK(cudaMemcpyAsync(s->sysdev.p, sd.data(), nsys * sizeof(SysDev), cudaMemcpyHostToDevice, st), "system table");
   SCK(cudaMemcpyAsync(s->cstart.p, cst.data(), nsys * 8, cudaMemcpyHostToDevice, st), "system table");
-  SCK(cudaMemcpyAsync(s->gstart.p, gst.data(), nsys * 8, cudaMemcpyHostToDevice, st), "system table");
-  SCK(cudaMemcpyAsync(s->ntot_dev.p, &ntot, 8, cudaMemcpyHostToDevice, st), "system table");
+  SCK(cudaMemcpyAsync(s->ntot_dev.p, &ntot, sizeof(ntot), cudaMemcpyHostToDevice, st), "system table");  // read by store/kick
 
   // ---- kick + drift, keys, sort, gather ----
   const SysDev *dsys = s->sysdev.as<SysDev>();
+  cudaEventRecord(c->ev[12], st);
   k_srv_expand<<<grid_for(ntot, 256), 256, 0, st>>>(ntot, nsys, dsys, s->cstart.as<int64_t>(), s->c2p.as<int64_t>(),
                                                     s->csys.as<int32_t>());
   k_srv_pre<<<grid_for(ntot, 256), 256, 0, st>>>(ntot, dsys, s->c2p.as<int64_t>(), s->csys.as<int32_t>(), s->pos.as<double4>(),
@@ -607,8 +598,7 @@ int32_t gpugrav_serve_tick(gpugrav_serve *s, int32_t *n_active)
      c->s_ix.ensure(ntot * 8) != cudaSuccess || c->s_iy.ensure(ntot * 8) != cudaSuccess || c->s_iz.ensure(ntot * 8) != cudaSuccess ||
      c->s_st.ensure(ntot + 16) != cudaSuccess || c->m_sys.ensure(ntot * 4) != cudaSuccess ||
      c->oldacc_s.ensure(ntot * 4) != cudaSuccess || c->acc_s.ensure(ntot * 24) != cudaSuccess ||
-     c->pot_s.ensure(ntot * 8) != cudaSuccess || c->nint_s.ensure(ntot * 4) != cudaSuccess ||
-     c->m_groups.ensure((size_t)ng * sizeof(int4)) != cudaSuccess)
+     c->pot_s.ensure(ntot * 8) != cudaSuccess || c->nint_s.ensure(ntot * 4) != cudaSuccess)
     return sfail(s, GPUGRAV_ERR_OOM, "tick buffers");
   k_srv_extent<<<nsys, 256, 0, st>>>(nsys, dsys, s->c2p.as<int64_t>(), s->pos.as<double4>(), c->m_doms.as<gpugrav_domain>());
   k_srv_keys<<<grid_for(ntot, 256), 256, 0, st>>>(ntot, s->csys.as<int32_t>(), s->c2p.as<int64_t>(), s->pos.as<double4>(),
@@ -628,13 +618,11 @@ int32_t gpugrav_serve_tick(gpugrav_serve *s, int32_t *n_active)
                                                     c->s_ix.as<uint64_t>(), c->s_iy.as<uint64_t>(), c->s_iz.as<uint64_t>(),
                                                     c->s_st.as<uint8_t>(), c->m_sys.as<int32_t>(), s->s2p.as<int64_t>(),
                                                     c->oldacc_s.as<float>());
-  k_srv_groups<<<grid_for(ng, 256), 256, 0, st>>>((int)ng, nsys, dsys, s->gstart.as<int64_t>(), c->m_groups.as<int4>());
   SCK(cudaGetLastError(), "tick kernels");
 
   // ---- batched build over all systems ----
   c->n          = ntot;
   c->ntop       = nsys;
-  c->m_ngroups  = (int32_t)ng;
   c->built      = false;
   c->layout32_valid = false;
   int bstat = 0;
@@ -647,23 +635,65 @@ int32_t gpugrav_serve_tick(gpugrav_serve *s, int32_t *n_active)
   WalkConst wc;
   make_walk_const(s->prm, &wc);
   c->want_pot = false;
-  std::vector<void *> ptrs = {c->g_sm.p,  c->g_rel.p,  c->g_kids.p,  c->g_pm.p,  c->g_pst.p,  c->s_pm.p,   c->s_st.p,
-                              c->oldacc_s.p, c->m_groups.p, c->g_stack.p, c->acc_s.p, c->nint_s.p, c->scratch.p, c->counters.p,
-                              c->m_sys.p,  s->s2p.p};
-  (void)ptrs;
-  SCK(cudaMemsetAsync(c->counters.as<int>() + 14, 0, 4, st), "walk flags");
-  SCK(gg::walk32_stage(c, wc), "walk");
-  k_srv_post<<<grid_for(ntot, 256), 256, 0, st>>>(s->ntot_dev.as<int64_t>(), c->m_sys.as<int32_t>(), dsys, s->s2p.as<int64_t>(),
-                                                  c->acc_s.as<double>(), s->vel.as<double4>(), s->acc.as<double4>(),
-                                                  s->oldacc.as<float>());
-  int walk_err = 0;
+  cudaEventRecord(c->ev[13], st);
+  SCK(gg::walk32_prepare(c, wc), "walk");
+  // Every pointer and launch parameter the captured nodes hold; the counts they depend on
+  // (particles, groups) are read from device memory, so one graph serves every tick
+  // until a buffer is reallocated.
+  const std::vector<const void *> key = {c->g_sm.p,     c->g_rel.p,    c->g_kids.p,   c->g_pm.p,          c->g_pst.p,
+                                         c->s_pm.p,     c->s_st.p,     c->oldacc_s.p, c->g_groups.p,      c->g_stack.p,
+                                         c->acc_s.p,    c->pot_s.p,    c->nint_s.p,   c->scratch.p,       c->counters.p,
+                                         c->m_sys.p,    s->s2p.p,      s->sysdev.p,   s->ntot_dev.p,      s->vel.p,
+                                         s->acc.p,      s->oldacc.p,   c->g_ngroups.p, c->w32_kernel,
+                                         (const void *)(intptr_t)c->w32_blocks};
+  if(!s->graph || key != s->graph_key)
+    {
+      if(s->graph)
+        {
+          cudaGraphExecDestroy(s->graph);
+          s->graph = nullptr;
+        }
+      cudaGraph_t g = nullptr;
+      SCK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "capture");
+      cudaError_t e1 = cudaMemsetAsync(c->counters.as<int>() + 14, 0, 4, st);
+      k_srv_bh<<<148 * 4, 256, 0, st>>>(c->g_ngroups.as<int>(), dsys, c->g_groups.as<int4>());
+      cudaError_t e2 = gg::walk32_launch(c);
+      k_srv_post<<<148 * 8, 256, 0, st>>>(s->ntot_dev.as<int64_t>(), c->m_sys.as<int32_t>(), dsys, s->s2p.as<int64_t>(),
+                                          c->acc_s.as<double>(), s->vel.as<double4>(), s->acc.as<double4>(), s->oldacc.as<float>());
+      cudaError_t e3 = cudaGetLastError();
+      cudaError_t e4 = cudaStreamEndCapture(st, &g);
+      SCK(e1 != cudaSuccess ? e1 : e2 != cudaSuccess ? e2 : e3 != cudaSuccess ? e3 : e4, "capture");
+      cudaError_t e5 = cudaGraphInstantiate(&s->graph, g, 0);
+      cudaGraphDestroy(g);
+      if(e5 != cudaSuccess)
+        s->graph = nullptr;
+      SCK(e5, "graph instantiate");
+      s->graph_key = key;
+      s->graph_captures++;
+    }
+  cudaEventRecord(c->ev[14], st);
+  SCK(cudaGraphLaunch(s->graph, st), "walk graph");
+  cudaEventRecord(c->ev[15], st);
+  s->graph_replays++;
+  int walk_err                = 0;
+  unsigned long long inter    = 0;
   SCK(cudaMemcpyAsync(&walk_err, c->counters.as<int>() + 14, 4, cudaMemcpyDeviceToHost, st), "walk flags");
+  SCK(cudaMemcpyAsync(&inter, c->counters.as<int>() + 32, 8, cudaMemcpyDeviceToHost, st), "walk flags");
+  SCK(cudaMemsetAsync(c->counters.as<int>() + 32, 0, 8, st), "walk flags");
   SCK(cudaStreamSynchronize(st), "tick");
   if(walk_err)
     return sfail(s, GPUGRAV_ERR_DEEP_TREE, "walk stack exhausted");
 
   // ---- state machine, completion ----
   const double t_end = now_s();
+  {
+    float b = 0, w = 0;
+    cudaEventElapsedTime(&b, c->ev[12], c->ev[13]);
+    cudaEventElapsedTime(&w, c->ev[14], c->ev[15]);
+    s->stats.build_s += 1e-3 * b;
+    s->stats.walk_s += 1e-3 * w;
+    s->stats.interactions += (int64_t)inter;
+  }
   std::vector<gpugrav_serve::Req *> keep;
   for(auto *r : s->active)
     {
@@ -707,10 +737,13 @@ int32_t gpugrav_serve_tick(gpugrav_serve *s, int32_t *n_active)
       s->stats.completed++;
     }
   s->active.swap(keep);
+  s->stats.finish_s += now_s() - t_end;
   s->stats.ticks++;
   s->stats.last_tick_s      = t_end - t_tick;
   s->stats.last_tick_particles = ntot;
   s->stats.last_tick_systems   = nsys;
+  s->stats.graph_captures      = s->graph_captures;
+  s->stats.graph_replays       = s->graph_replays;
   return GPUGRAV_OK;
 }
 

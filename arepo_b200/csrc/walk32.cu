@@ -48,6 +48,13 @@ constexpr int kUnroll  = GG_W32_UNROLL;   // list entries in flight per lane in 
 // added at most 32 per round and the list is evaluated first whenever a round could overflow it
 constexpr int kListCap = kEvalAt + 64;
 constexpr int kStackCap = 16384;  // traversal stack entries per warp (global memory)
+// A node that the group-box test opens although it is smaller than 1/kVote of the box's largest side
+// and nearer to the box than that is tested against every target of the group instead (opened
+// only if some target's own criterion opens it).  For a compact group this never happens; for a
+// group whose targets are far apart (outskirts of an isolated system, where consecutive targets
+// in key order can lie on both sides of a dense core) the box test alone would open the whole
+// core down to single particles.
+constexpr float kVote = 16.0f;
 
 #define SF1 10.666666666667f
 #define SF2 32.0f
@@ -338,7 +345,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                                                         const int4 *__restrict__ g_kids, const double4 *__restrict__ g_pm,
                                                         const uint8_t *__restrict__ g_pst, const double4 *__restrict__ tpm,
                                                         const uint8_t *__restrict__ tst, const float *__restrict__ oldacc,
-                                                        int64_t n, int ngroups, const int4 *__restrict__ groups,
+                                                        const int *__restrict__ ngroups_dev, const int4 *__restrict__ groups,
                                                         const W32Const *__restrict__ wcp,
                                                         int *__restrict__ stack_base, int *__restrict__ work,
                                                         double *__restrict__ acc_out, double *__restrict__ pot_out,
@@ -359,6 +366,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
   float4 *LP             = il_p[warp];
   float *LH              = il_h[warp];
   unsigned long long my_total = 0;
+  const int ng           = *ngroups_dev;  // device-side count: no host round trip, graph replays
 
   while(true)
     {
@@ -366,40 +374,31 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
       if(lane == 0)
         grp = atomicAdd(work, 1);
       grp = __shfl_sync(0xffffffffu, grp, 0);
-      if(grp >= ngroups)
+      if(grp >= ng)
         break;
+      // group of up to 32*TPL consecutive targets; lane holds targets t0 + lane + 32k.  A group lies
+      // inside one system and walks that system's tree (root).
+      const int4 G       = groups[grp];
+      const int64_t t0   = G.x;
+      const int cnt      = G.y;
+      const int root     = G.z;
+      const int bh       = G.w >= 0 ? G.w : w.bh;
       WALK_STAT(3, 1);
-      // group of up to 32*TPL consecutive targets; lane holds targets t0 + lane + 32k.  With a group
-      // table (several systems) a group lies inside one system and walks that system's tree.
-      int64_t t0, tend;
-      int root = 0, bh = w.bh;
-      if(groups)
-        {
-          const int4 G = groups[grp];
-          t0           = G.x;
-          tend         = (int64_t)G.x + G.y;
-          root         = G.z;
-          bh           = G.w;
-        }
-      else
-        {
-          t0   = (int64_t)grp * 32 * TPL;
-          tend = t0 + 32 * TPL < n ? t0 + 32 * TPL : n;
-        }
       double4 p[TPL];
       double mnx = 1e300, mxx = -1e300, mny = 1e300, mxy = -1e300, mnz = 1e300, mxz = -1e300;
-      float hmin_l = 3.0e38f, amin_l = 3.0e38f;
+      float hmin_l = 3.0e38f, amin_l = 3.0e38f, a_l[TPL];
 #pragma unroll
       for(int k = 0; k < TPL; k++)
         {
-          const int64_t t  = t0 + lane + 32 * k;
-          const int64_t tt = t < tend ? t : t0;  // idle slots repeat the group's first target
+          const int s      = lane + 32 * k;
+          const int64_t tt = t0 + (s < cnt ? s : 0);  // idle slots repeat the group's first target
           p[k]             = tpm[tt];
+          a_l[k]           = w.erracc * oldacc[tt];
           mnx = fmin(mnx, p[k].x), mxx = fmax(mxx, p[k].x);
           mny = fmin(mny, p[k].y), mxy = fmax(mxy, p[k].y);
           mnz = fmin(mnz, p[k].z), mxz = fmax(mxz, p[k].z);
           hmin_l = fminf(hmin_l, w.soft[tst[tt]]);
-          amin_l = fminf(amin_l, w.erracc * oldacc[tt]);
+          amin_l = fminf(amin_l, a_l[k]);
         }
       // group box (FP64), centre g, half extent (rounded up)
       mnx = wmin(mnx), mxx = wmax(mxx), mny = wmin(mny), mxy = wmax(mxy), mnz = wmin(mnz), mxz = wmax(mxz);
@@ -408,14 +407,15 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                   ez = (float)(0.5 * (mxz - mnz)) * 1.000001f;
       const float h_min    = wminf(hmin_l);
       const float aold_min = wminf(amin_l);
+      // box side squared over kVote^2: a node smaller than this and closer than it gets the per-target vote
+      const float side     = 2.0f * fmaxf(ex, fmaxf(ey, ez));
+      const float vote_r2  = side * side * (1.0f / (kVote * kVote));
       Tgt T[TPL];
 #pragma unroll
       for(int k = 0; k < TPL; k++)
         {
-          const int64_t t  = t0 + lane + 32 * k;
-          const int64_t tt = t < tend ? t : t0;
           T[k].x = (float)(p[k].x - gx), T[k].y = (float)(p[k].y - gy), T[k].z = (float)(p[k].z - gz);
-          T[k].h  = w.soft[tst[tt]];
+          T[k].h  = w.soft[tst[t0 + (lane + 32 * k < cnt ? lane + 32 * k : 0)]];
           T[k].ax = T[k].ay = T[k].az = T[k].pot = 0.0f;
           T[k].dax = T[k].day = T[k].daz = T[k].dpot = 0.0;
           T[k].ni = 0;
@@ -440,6 +440,8 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
           float4 entry = make_float4(0, 0, 0, 0);
           float hj     = 0;
           int fc = 0, fp = 0, nc = 0, np = 0;
+          bool vote = false, vote_keep = false;  // per-target vote pending; entry kept if accepted
+          float4 vrel = make_float4(0, 0, 0, 0);   // centre - CoM, side of a voting node
           if(node >= 0)
             {
               const double4 sm = g_sm[node];
@@ -479,6 +481,13 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                           fp     = kd.y;
                           nc     = kd.z & 15;
                           np     = (kd.z >> 4) & 15;
+                          if(L2 < vote_r2 && rmin2 < vote_r2)
+                            {
+                              vote      = true;
+                              vote_keep = !PERIODIC || rmin2 < w.rcut2;
+                              vrel      = rel;
+                              entry     = make_float4(sx, sy, sz, m);
+                            }
                         }
                       else if(!PERIODIC || rmin2 < w.rcut2)
                         {
@@ -487,6 +496,40 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                           entry  = make_float4(sx, sy, sz, m);
                         }
                     }
+                }
+            }
+          // per-target vote: the node stays open only if some target's own criterion opens it
+          if(__ballot_sync(0xffffffffu, vote))
+            {
+              bool need    = false;
+              const float L = vrel.w, L2 = L * L;
+#pragma unroll
+              for(int k = 0; k < TPL; k++)
+                for(int i = 0; i < 32; i++)
+                  {
+                    const float tx = __shfl_sync(0xffffffffu, T[k].x, i), ty = __shfl_sync(0xffffffffu, T[k].y, i),
+                                tz = __shfl_sync(0xffffffffu, T[k].z, i), th = __shfl_sync(0xffffffffu, T[k].h, i),
+                                ta = __shfl_sync(0xffffffffu, a_l[k], i);
+                    if(vote && !need && i + 32 * k < cnt)
+                      {
+                        const float dx = entry.x - tx, dy = entry.y - ty, dz = entry.z - tz;
+                        const float r2 = dx * dx + dy * dy + dz * dz;
+                        bool o;
+                        if(bh)
+                          o = L2 > r2 * w.theta2;
+                        else
+                          o = (L2 > r2 * 1.44f) || (entry.w * L2 > r2 * r2 * ta) ||
+                              (fabsf(entry.x + vrel.x - tx) < 0.6f * L && fabsf(entry.y + vrel.y - ty) < 0.6f * L &&
+                               fabsf(entry.z + vrel.z - tz) < 0.6f * L);
+                        if(!o && hj > th && r2 < hj * hj)
+                          o = true;
+                        need = o;
+                      }
+                  }
+              if(vote && !need)
+                {
+                  action = vote_keep ? 1 : 0;
+                  nc = np = 0;
                 }
             }
           // accepted nodes -> list
@@ -583,8 +626,9 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
 #pragma unroll
       for(int k = 0; k < TPL; k++)
         {
-          const int64_t t = t0 + lane + 32 * k;
-          if(t < tend)
+          const int s     = lane + 32 * k;
+          const int64_t t = t0 + s;
+          if(s < cnt)
             {
               acc_out[3 * t + 0] = T[k].dax;
               acc_out[3 * t + 1] = T[k].day;
@@ -601,6 +645,98 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
   if(lane == 0 && my_total)
     atomicAdd(total, my_total);
 }
+
+// ---- walk groups -------------------------------------------------------------------------
+// A group is up to `cap` consecutive targets in Peano-Hilbert order, never spanning two systems.
+// cd[i] is the depth of the deepest cell holding particles i and i+1 (-1 across systems and after
+// the last particle).  Optionally (slack < 64) groups are also cut between tree cells: pd[i] is the
+// depth of the deepest cell around particle i that holds more than cap particles (-1: its whole
+// system fits in one group), and consecutive particles stay in one group only while each lies
+// inside the other's pd cell (up to `slack` levels above it).  Cell cuts bound a group's box by a
+// tree cell at the price of partly filled warps; the per-target vote of the walk already removes
+// the cost of loose groups, and plain key-order groups are faster on the measured workloads.
+__global__ void k_grp_pd(int64_t n, const int8_t *__restrict__ cd, int cap, int8_t *__restrict__ pd)
+{
+  for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    {
+      int64_t l = i, r = i;  // current cell [l, r]
+      int res   = -1;
+      while(true)
+        {
+          const int dl = l > 0 ? cd[l - 1] : -1;
+          const int dr = cd[r];
+          const int d  = dl > dr ? dl : dr;  // depth of the next larger cell
+          if(d < 0)
+            break;
+          bool over = false;
+          while(l > 0 && cd[l - 1] >= d)
+            if(r - --l + 1 > cap)
+              {
+                over = true;
+                break;
+              }
+          while(!over && cd[r] >= d)
+            if(++r - l + 1 > cap)
+              over = true;
+          if(over)
+            {
+              res = d;
+              break;
+            }
+        }
+      pd[i] = (int8_t)res;
+    }
+}
+
+// segment start candidates: i where a group must begin (system start or a cut before i)
+__global__ void k_grp_cut(int64_t n, const int8_t *__restrict__ cd, const int8_t *__restrict__ pd, int slack,
+                          int32_t *__restrict__ segv)
+{
+  for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    {
+      bool cut = (i == 0);
+      if(!cut)
+        {
+          const int c = cd[i - 1];
+          cut         = c < 0;
+          if(pd && !cut)
+            {
+              const int p = pd[i - 1] > pd[i] ? pd[i - 1] : pd[i];
+              cut         = c < p - slack;
+            }
+        }
+      segv[i] = cut ? (int32_t)i : 0;
+    }
+}
+
+__global__ void k_grp_start(int64_t n, const int32_t *__restrict__ seg, int cap, int32_t *__restrict__ flag)
+{
+  for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    flag[i] = ((i - seg[i]) % cap == 0) ? 1 : 0;
+}
+
+// group table: (first target, count, root node, -1 = criterion of the walk constants)
+__global__ void k_grp_fill(int64_t n, const int32_t *__restrict__ flag, const int32_t *__restrict__ gid, int cap,
+                           const int32_t *__restrict__ sys, int4 *__restrict__ groups, int *__restrict__ ngroups)
+{
+  for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    {
+      if(flag[i])
+        {
+          int cnt = 1;
+          while(cnt < cap && i + cnt < n && !flag[i + cnt])
+            cnt++;
+          groups[gid[i]] = make_int4((int)i, cnt, sys ? sys[i] : 0, -1);
+        }
+      if(i == n - 1)
+        *ngroups = gid[i] + flag[i];
+    }
+}
+
+struct MaxOp32
+{
+  __device__ __forceinline__ int32_t operator()(int32_t a, int32_t b) const { return a > b ? a : b; }
+};
 
 int grid_for(int64_t n, int threads)
 {
@@ -643,6 +779,42 @@ void make_w32(const WalkConst &wc, W32Const *w)
         return _e;            \
     }                         \
   while(0)
+
+// walk group table of the current tree (see k_grp_pd); the group count stays on the device
+cudaError_t groups_stage(gpugrav_ctx *c)
+{
+  const int64_t n = c->n;
+  cudaStream_t st = c->stream;
+  const int cap   = 32 * ((c->walk32_tpl == 1 || c->multi) ? 1 : 2);
+  GG_TRY(c->g_groups.ensure(n * sizeof(int4)));
+  GG_TRY(c->g_ngroups.ensure(16));
+  GG_TRY(c->g_gpd.ensure(n + 16));
+  GG_TRY(c->g_gseg.ensure(n * 4));
+  GG_TRY(c->g_gflag.ensure(n * 4));
+  GG_TRY(c->g_gid.ensure(n * 4));
+  GG_TRY(cudaMemsetAsync(c->g_ngroups.p, 0, sizeof(int), st));
+  if(n == 0)
+    return cudaSuccess;
+  const bool cells = c->group_slack < 64;  // otherwise: cut at system starts only
+  if(cells)
+    k_grp_pd<<<grid_for(n, 256), 256, 0, st>>>(n, c->s_cd.as<int8_t>(), cap, c->g_gpd.as<int8_t>());
+  k_grp_cut<<<grid_for(n, 256), 256, 0, st>>>(n, c->s_cd.as<int8_t>(), cells ? c->g_gpd.as<int8_t>() : nullptr,
+                                               c->group_slack, c->g_gflag.as<int32_t>());
+  size_t tb = 0;
+  GG_TRY(cub::DeviceScan::InclusiveScan(nullptr, tb, c->g_gflag.as<int32_t>(), c->g_gseg.as<int32_t>(), MaxOp32(), (int)n, st));
+  GG_TRY(c->sort_tmp.ensure(tb));
+  GG_TRY(cub::DeviceScan::InclusiveScan(c->sort_tmp.p, tb, c->g_gflag.as<int32_t>(), c->g_gseg.as<int32_t>(), MaxOp32(), (int)n,
+                                        st));
+  k_grp_start<<<grid_for(n, 256), 256, 0, st>>>(n, c->g_gseg.as<int32_t>(), cap, c->g_gflag.as<int32_t>());
+  tb = 0;
+  GG_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, c->g_gflag.as<int32_t>(), c->g_gid.as<int32_t>(), (int)n, st));
+  GG_TRY(c->sort_tmp.ensure(tb));
+  GG_TRY(cub::DeviceScan::ExclusiveSum(c->sort_tmp.p, tb, c->g_gflag.as<int32_t>(), c->g_gid.as<int32_t>(), (int)n, st));
+  k_grp_fill<<<grid_for(n, 256), 256, 0, st>>>(n, c->g_gflag.as<int32_t>(), c->g_gid.as<int32_t>(), cap,
+                                                c->multi ? c->m_sys.as<int32_t>() : nullptr, c->g_groups.as<int4>(),
+                                                c->g_ngroups.as<int>());
+  return cudaGetLastError();
+}
 
 // breadth-first node layout + particles grouped by parent (built once per tree)
 cudaError_t layout32_stage(gpugrav_ctx *c)
@@ -688,47 +860,66 @@ cudaError_t layout32_stage(gpugrav_ctx *c)
   GG_TRY(cudaStreamSynchronize(st));
   if(e)
     return cudaErrorUnknown;
+  GG_TRY(groups_stage(c));
   c->layout32_valid = true;
   return cudaSuccess;
 }
 
-cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc)
+typedef decltype(&k_walk32<true, true, 1>) Walk32Kernel;
+
+// Everything that must happen before the walk launch and may not be captured in a graph
+// (layout, constants upload from host memory, stack allocation, launch shape).
+cudaError_t walk32_prepare(gpugrav_ctx *c, const WalkConst &wc)
 {
   if(!c->layout32_valid)
     GG_TRY(layout32_stage(c));
   cudaStream_t st = c->stream;
-  const int64_t n = c->n;
   W32Const w;
   make_w32(wc, &w);
-  // constants live after the per-warp stacks' bookkeeping in the scratch buffer
   GG_TRY(c->scratch.ensure(sizeof(W32Const) + 256));
   GG_TRY(cudaMemcpyAsync(c->scratch.p, &w, sizeof(w), cudaMemcpyHostToDevice, st));
+  GG_TRY(cudaStreamSynchronize(st));  // `w` lives on this stack frame
   int dev = 0, sms = 0, per_sm = 0;
   GG_TRY(cudaGetDevice(&dev));
   GG_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const bool periodic = wc.periodic != 0;
   const bool pot      = c->want_pot;
   const int tpl       = (c->walk32_tpl == 1 || c->multi) ? 1 : 2;
-  auto kern = tpl == 2 ? (periodic ? (pot ? k_walk32<true, true, 2> : k_walk32<true, false, 2>)
-                                   : (pot ? k_walk32<false, true, 2> : k_walk32<false, false, 2>))
-                       : (periodic ? (pot ? k_walk32<true, true, 1> : k_walk32<true, false, 1>)
-                                   : (pot ? k_walk32<false, true, 1> : k_walk32<false, false, 1>));
+  Walk32Kernel kern = tpl == 2 ? (periodic ? (pot ? k_walk32<true, true, 2> : k_walk32<true, false, 2>)
+                                           : (pot ? k_walk32<false, true, 2> : k_walk32<false, false, 2>))
+                               : (periodic ? (pot ? k_walk32<true, true, 1> : k_walk32<true, false, 1>)
+                                           : (pot ? k_walk32<false, true, 1> : k_walk32<false, false, 1>));
   GG_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * kWarps, 0));
   if(per_sm < 1)
     per_sm = 1;
-  const int blocks  = sms * per_sm;
-  const int ngroups = c->multi ? c->m_ngroups : (int)((n + 32 * tpl - 1) / (32 * tpl));
-  GG_TRY(c->g_stack.ensure((size_t)blocks * kWarps * kStackCap * sizeof(int)));
-  int *work = c->counters.as<int>() + 20;
-  int *err  = c->counters.as<int>() + 14;
+  c->w32_kernel = (void *)kern;
+  c->w32_blocks = sms * per_sm;
+  GG_TRY(c->g_stack.ensure((size_t)c->w32_blocks * kWarps * kStackCap * sizeof(int)));
+  return cudaSuccess;
+}
+
+// The walk itself: counter reset + one persistent launch (capturable).  The group table and
+// its count live in device memory, so a captured launch serves every tree of the same buffers.
+cudaError_t walk32_launch(gpugrav_ctx *c)
+{
+  cudaStream_t st = c->stream;
+  int *work       = c->counters.as<int>() + 20;
+  int *err        = c->counters.as<int>() + 14;
   GG_TRY(cudaMemsetAsync(work, 0, sizeof(int), st));
-  kern<<<blocks, 32 * kWarps, 0, st>>>(c->g_sm.as<double4>(), c->g_rel.as<float4>(), c->g_kids.as<int4>(), c->g_pm.as<double4>(),
-                                       c->g_pst.as<uint8_t>(), c->s_pm.as<double4>(), c->s_st.as<uint8_t>(),
-                                       c->oldacc_s.as<float>(), n, ngroups, c->multi ? c->m_groups.as<int4>() : nullptr,
-                                       (const W32Const *)c->scratch.p, c->g_stack.as<int>(),
-                                       work, c->acc_s.as<double>(), c->pot_s.as<double>(), c->nint_s.as<int32_t>(),
-                                       (unsigned long long *)(c->counters.as<int>() + 32), err);
+  Walk32Kernel kern = (Walk32Kernel)c->w32_kernel;
+  kern<<<c->w32_blocks, 32 * kWarps, 0, st>>>(c->g_sm.as<double4>(), c->g_rel.as<float4>(), c->g_kids.as<int4>(),
+                                              c->g_pm.as<double4>(), c->g_pst.as<uint8_t>(), c->s_pm.as<double4>(),
+                                              c->s_st.as<uint8_t>(), c->oldacc_s.as<float>(), c->g_ngroups.as<int>(),
+                                              c->g_groups.as<int4>(), (const W32Const *)c->scratch.p,
+                                              c->g_stack.as<int>(), work, c->acc_s.as<double>(), c->pot_s.as<double>(),
+                                              c->nint_s.as<int32_t>(), (unsigned long long *)(c->counters.as<int>() + 32), err);
   return cudaGetLastError();
+}
+
+cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc)
+{
+  GG_TRY(walk32_prepare(c, wc));
+  return walk32_launch(c);
 }
 }  // namespace gg
 

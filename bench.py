@@ -21,6 +21,18 @@ With --gpus N (torchrun, one process per GPU) every rank runs its own
 independent zoom box (seed + rank): replicas, weak scaling, no collective on
 the data path; the step time is the maximum over ranks.
 
+Serving leg (rank 0 at N=1; --no-serving skips it): a seeded stream of isolated
+systems (Plummer spheres and Hernquist haloes, 50/50, N log-uniform in
+[10^3, 10^6], G=1, softening 0.02 scale radius, FP32 walk, ErrTolForceAcc 0.0025),
+each running the first-step sequence (Barnes-Hut pass, relative pass) and K=16
+kick-drift-kick steps of dt=0.005 under a 120 GB admission budget.  Throughput
+(requests/s, particle-steps/s) all-arrived-at-once for the continuously batched
+server and for one-request-at-a-time execution (max_systems=1) on the same
+requests; p50/p99 latency under Poisson arrivals at a fraction of the batched
+capacity.  Wall clock of the host-driven serving loop: admission uploads, every
+tick's kernels and result downloads are inside it.  --serve-requests 10000 runs
+the full stream.
+
 --impl reference times the reference's own C (oracle/_ref, compiled from the
 reference sources) on the host cores on a bounded sample of the same workload.
 """
@@ -211,6 +223,105 @@ def reference_arm(args):
 
 
 # --------------------------------------------------------------------------------------
+# serving leg
+# --------------------------------------------------------------------------------------
+SERVE_NMIN, SERVE_NMAX = 1000, 1000000
+SERVE_EPS, SERVE_K, SERVE_DT = 0.02, 16, 0.005
+SERVE_BUDGET = 120e9
+
+
+def serving_stream(count: int, seed: int = 1005):
+    """Sizes (log-uniform in [SERVE_NMIN, SERVE_NMAX]) and kinds (0 Plummer, 1 Hernquist) of the stream."""
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(SERVE_NMIN), np.log(SERVE_NMAX), count)).astype(np.int64)
+    return ns, rng.integers(0, 2, count)
+
+
+def serving_system(n: int, kind: int, seed: int):
+    from arepo_b200 import ics
+
+    ic = ics.plummer(n, seed, eps=SERVE_EPS) if kind == 0 else ics.hernquist(n, seed=seed, eps=SERVE_EPS)
+    return ic["pos"], np.zeros_like(ic["pos"]), ic["mass"], ic["softtype"]
+
+
+def run_stream(systems, ids, arrivals, max_systems, device, max_particles):
+    """Serve requests `ids` (arrival offsets in seconds, or None: all at once) and return throughput
+    and latency figures. Latency runs from the scheduled arrival to the poll that returned the result."""
+    from arepo_b200.serving import GravityServer, serving_params
+
+    prm = serving_params(SERVE_EPS)
+    warm = serving_system(2000, 0, 99)
+    with GravityServer(prm, device=device, max_systems=max_systems, max_particles=max_particles,
+                       budget_bytes=SERVE_BUDGET) as srv:
+        for w in range(2):  # warm-up: first buffers, graph capture
+            srv.submit((1 << 40) + w, *warm, nsteps=1, dt=SERVE_DT)
+        srv.run_to_completion()
+        s0 = srv.stats()
+        arrive, lat, svc, sizes = {}, [], [], []
+        k, nsys_ticks = 0, 0
+        t0 = time.monotonic()
+        while True:
+            now = time.monotonic() - t0
+            while k < len(ids) and (arrivals is None or arrivals[k] <= now):
+                i = int(ids[k])
+                arrive[i] = t0 + (0.0 if arrivals is None else float(arrivals[k]))
+                srv.submit(i, *systems[i], nsteps=SERVE_K, dt=SERVE_DT)
+                k += 1
+            if not srv.busy():
+                if k >= len(ids):
+                    break
+                time.sleep(max(0.0, float(arrivals[k]) - (time.monotonic() - t0)))
+                continue
+            srv.tick()
+            nsys_ticks += srv.stats().last_tick_systems
+            for r in srv.poll_all():
+                lat.append(time.monotonic() - arrive[r.id])
+                svc.append(r.t_done - r.t_admit)
+                sizes.append(len(r.pos))
+        wall = time.monotonic() - t0
+        s1 = srv.stats()
+    ticks = s1.ticks - s0.ticks
+    return {"requests": len(ids), "wall_s": wall, "requests_per_s": len(ids) / wall,
+            "particle_steps_per_s": (s1.particle_steps - s0.particle_steps) / wall,
+            "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+            "service_p50_s": float(np.percentile(svc, 50)), "service_p99_s": float(np.percentile(svc, 99)),
+            "ticks": int(ticks), "mean_systems_per_tick": nsys_ticks / max(ticks, 1),
+            "phase_s": {k: getattr(s1, k) - getattr(s0, k) for k in ("admit_s", "build_s", "walk_s", "finish_s")},
+            "interactions_per_particle_step": (s1.interactions - s0.interactions) / max(1, s1.particle_steps - s0.particle_steps),
+            "graph_captures": int(s1.graph_captures - s0.graph_captures),
+            "graph_replays": int(s1.graph_replays - s0.graph_replays)}
+
+
+def serving_leg(args, device):
+    ns, kinds = serving_stream(args.serve_requests)
+    t = time.time()
+    systems = [serving_system(int(ns[i]), int(kinds[i]), 5000 + i) for i in range(len(ns))]
+    log(f"serving: generated {len(ns)} systems ({int(ns.sum())} particles) in {time.time() - t:.1f}s")
+    pool = int(min(1 << 27, max(int(ns.sum()), SERVE_NMAX) + 4096))
+    ncmp = min(args.serve_compare, len(ns))
+    cmp_ids = np.arange(ncmp)
+    batched = run_stream(systems, cmp_ids, None, 4096, device, pool)
+    log(f"serving: batched {batched['requests_per_s']:.2f} req/s")
+    serial = run_stream(systems, cmp_ids, None, 1, device, pool)
+    log(f"serving: serial {serial['requests_per_s']:.2f} req/s")
+    rate = args.serve_load * batched["requests_per_s"]
+    arr = np.cumsum(np.random.default_rng(1006).exponential(1.0 / rate, len(ns)))
+    poisson = run_stream(systems, np.arange(len(ns)), arr, 4096, device, pool)
+    log(f"serving: poisson p50 {poisson['latency_p50_s']:.2f}s p99 {poisson['latency_p99_s']:.2f}s")
+    return {
+        "stream": f"{len(ns)} isolated systems, Plummer/Hernquist 50/50 (seeded), N log-uniform in "
+                  f"[{SERVE_NMIN}, {SERVE_NMAX}], G=1, softening {SERVE_EPS} scale radius, zero initial velocities, "
+                  f"BH pass + relative pass (ErrTolForceAcc 0.0025) + K={SERVE_K} KDK steps of dt={SERVE_DT}, "
+                  f"FP32 walk, {SERVE_BUDGET / 1e9:.0f} GB admission budget",
+        "particles": int(ns.sum()),
+        "compare": {"requests": int(ncmp), "arrivals": "all at t=0", "batched": batched, "serial_max_systems_1": serial,
+                    "throughput_ratio": batched["particle_steps_per_s"] / serial["particle_steps_per_s"]},
+        "poisson": dict(poisson, rate_per_s=rate, load=args.serve_load),
+        "clock": "host wall clock of the serving loop (uploads, ticks, downloads included)",
+    }
+
+
+# --------------------------------------------------------------------------------------
 # our arm
 # --------------------------------------------------------------------------------------
 def our_arm(args):
@@ -393,6 +504,10 @@ def our_arm(args):
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                                     "sample": f"unavailable: {e}"}
     tree.close()
+    del pos_d, mass_d, st_d, acc_d, pot_d, ni_d, oldacc_d
+    torch.cuda.empty_cache()
+    if rank == 0 and world == 1 and not args.no_serving:
+        line["serving"] = serving_leg(args, local)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -413,6 +528,12 @@ def main():
                          "error below 1e-3 on the zoom box (the metric's accuracy bar)")
     ap.add_argument("--log2-half", type=int, default=23, help="log2 of each species' count (23 -> N=2^24)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=160, help="requests in the Poisson serving stream")
+    ap.add_argument("--serve-compare", type=int, default=48,
+                    help="first requests of the stream timed batched and one at a time")
+    ap.add_argument("--serve-load", type=float, default=0.7,
+                    help="Poisson arrival rate as a fraction of the batched all-at-once request rate")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -238,13 +238,19 @@ typedef struct gpugrav_serve_stats
   int64_t last_tick_particles;
   int32_t last_tick_systems;
   int32_t pad;
+  int64_t graph_captures;  /* walk + store/kick captured as a CUDA graph (again after a buffer moved) */
+  int64_t graph_replays;   /* ticks that launched the captured graph */
+  /* cumulative seconds: admission (host packing + uploads), keys/sort/build/layout (device),
+   * walk + store/kick (device), completion (downloads + unpacking) */
+  double admit_s, build_s, walk_s, finish_s;
+  int64_t interactions;  /* particle-node and particle-particle interactions of all walks */
 } gpugrav_serve_stats;
 
 int32_t gpugrav_serve_create(gpugrav_serve **srv, int32_t device, const gpugrav_params *params,
                              const gpugrav_serve_config *cfg);
 int32_t gpugrav_serve_destroy(gpugrav_serve *srv);
 const char *gpugrav_serve_last_error(gpugrav_serve *srv);
-/* host arrays, copied: pos, vel n*3; mass n; softtype n */
+/* host arrays, copied: pos, vel n*3; mass n; softtype n. id >= 0 (poll returns -1 for "none"). */
 int32_t gpugrav_serve_submit(gpugrav_serve *srv, int64_t id, int64_t n, const double *pos, const double *vel,
                              const double *mass, const uint8_t *softtype, int32_t nsteps, double dt);
 int32_t gpugrav_serve_cancel(gpugrav_serve *srv, int64_t id);

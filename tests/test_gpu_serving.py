@@ -36,8 +36,11 @@ def test_alone_equals_in_the_mix(cuda_lib):
         srv.tick()
         srv.submit(12, *_system("hernquist", 70000, 13), nsteps=2, dt=0.005)
         res = srv.run_to_completion()
+        st = srv.stats()
     mix = res[1]
     assert set(res) == {1, 10, 11, 12}
+    # the walk + store/kick graph is captured once per buffer layout and replayed otherwise
+    assert st.graph_replays == st.ticks and 1 <= st.graph_captures < st.ticks
     assert np.array_equal(mix.pos, alone.pos)
     assert np.array_equal(mix.vel, alone.vel)
     assert np.array_equal(mix.acc, alone.acc)
@@ -129,3 +132,5 @@ def test_submit_errors(cuda_lib):
         st2[0] = 3
         with pytest.raises(L.GpuGravError):
             srv.submit(3, pos, vel, mass, st2, nsteps=1, dt=0.01)
+        with pytest.raises(L.GpuGravError):  # -1 is poll's "no result"
+            srv.submit(-1, pos, vel, mass, st, nsteps=1, dt=0.01)
