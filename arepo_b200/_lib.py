@@ -127,6 +127,8 @@ class ServeStats(C.Structure):
         ("walk_s", C.c_double),
         ("finish_s", C.c_double),
         ("interactions", C.c_int64),
+        ("keys_s", C.c_double),
+        ("tree_s", C.c_double),
     ]
 
 

@@ -6,6 +6,7 @@
 //   gpugrav_walk   ~ gravity_tree(timebin)
 // Errors are returned as status codes (negative codes mirror force_treebuild_construct's);
 // nothing in the library exits.
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -19,15 +20,31 @@ using namespace gg;
 // ------------------------------------------------------------------------------
 // buffers
 // ------------------------------------------------------------------------------
+void gpugrav_ctx::mark(const char *what)
+{
+  if(!profile)
+    return;
+  cudaStreamSynchronize(stream);
+  const double t = std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  if(what && prof_t > 0)
+    prof[what] += t - prof_t;
+  prof_t = t;
+}
+
 cudaError_t gg::DevBuf::ensure(size_t bytes)
 {
   if(bytes <= cap && p)
     return cudaSuccess;
+  // a buffer that has to grow gets 25% headroom: sizes that drift upward from call to call (node
+  // counts of successive trees) would otherwise reallocate, and synchronise the device, every call
+  const bool regrow = p != nullptr;
   if(p)
     cudaFree(p);
   p   = nullptr;
   cap = 0;
   size_t want = bytes < 256 ? 256 : bytes;
+  if(regrow)
+    want += want / 4;
   want        = (want + 255) & ~(size_t)255;
   cudaError_t e = cudaMalloc(&p, want);
   if(e != cudaSuccess)
@@ -279,6 +296,8 @@ int32_t gpugrav_create(gpugrav_ctx **out, int32_t device, const gpugrav_params *
     c->walk32_tpl = atoi(e) == 1 ? 1 : 2;
   if(const char *e = getenv("GPUGRAV_GROUP_SLACK"))
     c->group_slack = atoi(e);
+  if(const char *e = getenv("GPUGRAV_PROFILE"))
+    c->profile = atoi(e) != 0;
   DeviceGuard g(device);
   if(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     {
@@ -306,6 +325,9 @@ int32_t gpugrav_destroy(gpugrav_ctx *c)
 {
   if(!c)
     return GPUGRAV_ERR_INVALID;
+  if(c->profile)
+    for(auto &kv : c->prof)
+      fprintf(stderr, "gpugrav profile %-24s %10.3f ms\n", kv.first.c_str(), 1e3 * kv.second);
   DeviceGuard g(c->device);
   cudaStreamSynchronize(c->stream);
   gg::DevBuf *bufs[] = {&c->bconst, &c->wconst, &c->pos_in, &c->mass_in, &c->st_in, &c->key, &c->key_alt, &c->idx, &c->perm,

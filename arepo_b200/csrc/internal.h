@@ -9,10 +9,21 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
 #include <string>
 #include <vector>
 
 #include "../../include/gpugrav.h"
+
+// return a failing CUDA status from a cudaError_t function
+#define GG_TRY(x)             \
+  do                          \
+    {                         \
+      cudaError_t _e = (x);   \
+      if(_e != cudaSuccess)   \
+        return _e;            \
+    }                         \
+  while(0)
 
 namespace gg
 {
@@ -83,6 +94,12 @@ struct gpugrav_ctx
   bool own_stream       = false;
   gpugrav_params prm{};
   std::string err;
+  // GPUGRAV_PROFILE=1: host wall time per build step (the stream is synchronised after each step),
+  // printed to stderr when the context is destroyed
+  bool profile = false;
+  std::map<std::string, double> prof;
+  double prof_t = 0;
+  void mark(const char *what);
 
   // ---- state ----
   int64_t n          = 0;
@@ -134,7 +151,7 @@ struct gpugrav_ctx
   gg::DevBuf scratch;                         // reductions
   gg::PinnedBuf pinned;
 
-  cudaEvent_t ev[16] = {};
+  cudaEvent_t ev[20] = {};
   gpugrav_timings timings{};
 };
 
@@ -152,6 +169,10 @@ cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc);
 cudaError_t walk32_prepare(gpugrav_ctx *c, const WalkConst &wc);
 cudaError_t walk32_launch(gpugrav_ctx *c);
 cudaError_t groups_stage(gpugrav_ctx *c);
+cudaError_t layout32_buffers(gpugrav_ctx *c, int64_t n, int64_t nn);
+cudaError_t layout32_reserve(gpugrav_ctx *c, int64_t n, int64_t nn);
+cudaError_t build_reserve(gpugrav_ctx *c, int64_t n, int64_t nn, int32_t ntop);
+cudaError_t node_arrays(gpugrav_ctx *c, int64_t nn);
 cudaError_t layout32_stage(gpugrav_ctx *c);
 cudaError_t direct_stage(gpugrav_ctx *c, const WalkConst &wc, int64_t nt, const int64_t *d_targets, int cut, double *d_acc,
                          double *d_pot);

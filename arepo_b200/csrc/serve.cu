@@ -19,6 +19,8 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <memory>
+#include <new>
 #include <vector>
 
 #include "internal.h"
@@ -101,54 +103,97 @@ __global__ void k_srv_pre(int64_t ntot, const SysDev *__restrict__ sys, const in
     }
 }
 
-// per-system extent (one block per system): isolated domain, 1.2 x the largest extent
+// Order-preserving map of a double onto an unsigned integer (for atomic min / max).
+__device__ __forceinline__ unsigned long long ord64(double x)
+{
+  const unsigned long long u = (unsigned long long)__double_as_longlong(x);
+  return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double unord64(unsigned long long u)
+{
+  return __longlong_as_double((long long)((u >> 63) ? (u & 0x7FFFFFFFFFFFFFFFull) : ~u));
+}
+
+// Extent of every system: blockIdx.y strides over the system's particles; partial boxes are
+// combined with atomics on ord64 values (ext: per system 3 minima then 3 maxima, preset by the host
+// to all-ones and zero).
 __global__ void k_srv_extent(int nsys, const SysDev *__restrict__ sys, const int64_t *__restrict__ c2p,
-                             const double4 *__restrict__ pos, gpugrav_domain *__restrict__ doms)
+                             const double4 *__restrict__ pos, unsigned long long *__restrict__ ext)
 {
   const int s = blockIdx.x;
   if(s >= nsys)
     return;
   double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-  for(int64_t i = threadIdx.x; i < sys[s].n; i += blockDim.x)
+  const int64_t n = sys[s].n, coff = sys[s].coff;
+  for(int64_t i = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.y * blockDim.x)
     {
-      double4 x = pos[c2p[sys[s].coff + i]];
+      const double4 x = pos[c2p[coff + i]];
       mn[0] = fmin(mn[0], x.x), mx[0] = fmax(mx[0], x.x);
       mn[1] = fmin(mn[1], x.y), mx[1] = fmax(mx[1], x.y);
       mn[2] = fmin(mn[2], x.z), mx[2] = fmax(mx[2], x.z);
     }
-  __shared__ double red[6][256];
   for(int j = 0; j < 3; j++)
+    for(int o = 16; o > 0; o >>= 1)
+      {
+        mn[j] = fmin(mn[j], __shfl_xor_sync(0xffffffffu, mn[j], o));
+        mx[j] = fmax(mx[j], __shfl_xor_sync(0xffffffffu, mx[j], o));
+      }
+  if((threadIdx.x & 31) == 0 && (int64_t)blockIdx.y * blockDim.x + threadIdx.x < n)
+    for(int j = 0; j < 3; j++)
+      {
+        atomicMin(&ext[6 * s + j], ord64(mn[j]));
+        atomicMax(&ext[6 * s + 3 + j], ord64(mx[j]));
+      }
+}
+
+// domain of every system: cube of 1.2 times the largest extent around the box centre
+__global__ void k_srv_domains(int nsys, const unsigned long long *__restrict__ ext, gpugrav_domain *__restrict__ doms)
+{
+  for(int s = blockIdx.x * blockDim.x + threadIdx.x; s < nsys; s += gridDim.x * blockDim.x)
     {
-      red[j][threadIdx.x]     = mn[j];
-      red[3 + j][threadIdx.x] = mx[j];
-    }
-  __syncthreads();
-  for(int o = blockDim.x / 2; o > 0; o >>= 1)
-    {
-      if(threadIdx.x < o)
-        for(int j = 0; j < 3; j++)
-          {
-            red[j][threadIdx.x]     = fmin(red[j][threadIdx.x], red[j][threadIdx.x + o]);
-            red[3 + j][threadIdx.x] = fmax(red[3 + j][threadIdx.x], red[3 + j][threadIdx.x + o]);
-          }
-      __syncthreads();
-    }
-  if(threadIdx.x == 0)
-    {
-      double len = 0;
+      double lo[3], hi[3], len = 0;
       for(int j = 0; j < 3; j++)
-        len = fmax(len, red[3 + j][0] - red[j][0]);
+        {
+          lo[j] = unord64(ext[6 * s + j]);
+          hi[j] = unord64(ext[6 * s + 3 + j]);
+          len   = fmax(len, hi[j] - lo[j]);
+        }
       len = 1.2 * (len > 0 ? len : 1.0);
       gpugrav_domain d;
       for(int j = 0; j < 3; j++)
         {
-          d.center[j] = 0.5 * (red[j][0] + red[3 + j][0]);
+          d.center[j] = 0.5 * (lo[j] + hi[j]);
           d.corner[j] = d.center[j] - 0.5 * len;
         }
       d.len         = len;
       d.inverse_len = 1.0 / len;
       d.big_fac     = len / 4503599627370496.0;
       doms[s]       = d;
+    }
+}
+
+// admitted system: submitted arrays pos (3n) | vel (3n) | mass (n), softening types -> pool
+__global__ void k_srv_unpack(int64_t n, int64_t off, const double *__restrict__ in, const uint8_t *__restrict__ st,
+                             double4 *__restrict__ pos, double4 *__restrict__ vel, uint8_t *__restrict__ stype)
+{
+  for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    {
+      pos[off + i]   = make_double4(in[3 * i], in[3 * i + 1], in[3 * i + 2], in[6 * n + i]);
+      vel[off + i]   = make_double4(in[3 * (n + i)], in[3 * (n + i) + 1], in[3 * (n + i) + 2], 0.0);
+      stype[off + i] = st[i];
+    }
+}
+
+// finished systems: pool (double4) -> packed pos | vel | acc (3n doubles each) for one download
+__global__ void k_srv_pack(int64_t n, int64_t off, const double4 *__restrict__ pos, const double4 *__restrict__ vel,
+                           const double4 *__restrict__ acc, double *__restrict__ out)
+{
+  for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    {
+      const double4 p = pos[off + i], v = vel[off + i], a = acc[off + i];
+      out[3 * i + 0] = p.x, out[3 * i + 1] = p.y, out[3 * i + 2] = p.z;
+      out[3 * (n + i) + 0] = v.x, out[3 * (n + i) + 1] = v.y, out[3 * (n + i) + 2] = v.z;
+      out[3 * (2 * n + i) + 0] = a.x, out[3 * (2 * n + i) + 1] = a.y, out[3 * (2 * n + i) + 2] = a.z;
     }
 }
 
@@ -265,14 +310,13 @@ struct gpugrav_serve
     int64_t n  = 0;
     int32_t nsteps = 0;
     double dt      = 0;
-    std::vector<double> pos, vel, mass;
-    std::vector<uint8_t> st;
+    std::unique_ptr<double[]> in;  // pos (3n) | vel (3n) | mass (n), until admitted
+    std::unique_ptr<uint8_t[]> st;
     // running
     int32_t state = ST_NEW, steps_done = 0;
     int64_t pool_off = -1;
     double t_submit = 0, t_admit = 0, t_done = 0;
     // result
-    std::vector<double> out_pos, out_vel, out_acc;
   };
   std::deque<Req *> queue;       // waiting for admission (arrival order)
   std::vector<Req *> active;     // admitted, in admission order
@@ -282,7 +326,7 @@ struct gpugrav_serve
   int64_t bytes_per_particle = 0;
 
   gg::DevBuf pos, vel, acc, oldacc, stype;  // particle pool
-  gg::DevBuf sysdev, cstart, c2p, csys, s2p, ntot_dev;
+  gg::DevBuf sysdev, cstart, c2p, csys, s2p, ntot_dev, ext, up, dl;
   gg::PinnedBuf staging;
 
   // captured walk + store/kick graph; re-captured when a buffer it names moves
@@ -351,10 +395,42 @@ void pool_free(gpugrav_serve *s, int64_t off, int64_t n)
     }
 }
 
+cudaError_t serve_reserve(gpugrav_serve *s)
+{
+  gpugrav_ctx *c  = s->ctx;
+  const int64_t n = s->pool_cap;
+  const int nsys  = s->cfg.max_systems;
+  GG_TRY(c->m_doms.ensure((size_t)nsys * sizeof(gpugrav_domain)));
+  GG_TRY(c->key.ensure(n * sizeof(u128)));
+  GG_TRY(c->key_alt.ensure(n * sizeof(u128)));
+  GG_TRY(c->idx.ensure(n * 4));
+  GG_TRY(c->perm.ensure(n * 4));
+  GG_TRY(c->s_pm.ensure(n * sizeof(double4)));
+  GG_TRY(c->s_ix.ensure(n * 8));
+  GG_TRY(c->s_iy.ensure(n * 8));
+  GG_TRY(c->s_iz.ensure(n * 8));
+  GG_TRY(c->s_st.ensure(n + 16));
+  GG_TRY(c->m_sys.ensure(n * 4));
+  GG_TRY(c->oldacc_s.ensure(n * 4));
+  GG_TRY(c->acc_s.ensure(n * 24));
+  GG_TRY(c->pot_s.ensure(n * 8));
+  GG_TRY(c->nint_s.ensure(n * 4));
+  size_t tb = 0;
+  GG_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, c->key.as<u128>(), c->key_alt.as<u128>(), c->idx.as<uint32_t>(),
+                                         c->perm.as<uint32_t>(), (int)n, 0, 128, s->st));
+  GG_TRY(c->sort_tmp.ensure(tb));
+  GG_TRY(gg::build_reserve(c, n, n, nsys));
+  GG_TRY(gg::layout32_reserve(c, n, n));
+  GG_TRY(s->up.ensure((size_t)n * (7 * sizeof(double) + 1)));
+  return s->dl.ensure((size_t)n * 9 * sizeof(double));
+}
+
 int64_t in_flight(const gpugrav_serve *s)
 {
   int64_t t = 0;
   for(auto *r : s->active)
+    t += r->n;
+  for(auto *r : s->finished)  // results stay in the pool until polled
     t += r->n;
   return t;
 }
@@ -403,7 +479,8 @@ int32_t gpugrav_serve_create(gpugrav_serve **out, int32_t device, const gpugrav_
             s->sysdev.ensure((size_t)cfg->max_systems * sizeof(SysDev)) == cudaSuccess &&
             s->cstart.ensure((size_t)(cfg->max_systems + 1) * 8) == cudaSuccess &&
             s->c2p.ensure(s->pool_cap * 8) == cudaSuccess && s->csys.ensure(s->pool_cap * 4) == cudaSuccess &&
-            s->s2p.ensure(s->pool_cap * 8) == cudaSuccess && s->ntot_dev.ensure(64) == cudaSuccess;
+            s->s2p.ensure(s->pool_cap * 8) == cudaSuccess && s->ntot_dev.ensure(64) == cudaSuccess &&
+            s->ext.ensure((size_t)cfg->max_systems * 6 * 8) == cudaSuccess;
   // the build context's constants (isolated, softening table)
   if(ok)
     {
@@ -416,6 +493,9 @@ int32_t gpugrav_serve_create(gpugrav_serve **out, int32_t device, const gpugrav_
         bc.soft[i] = p.force_softening[i];
       ok = cudaMemcpy(ctx->bconst.p, &bc, sizeof(bc), cudaMemcpyHostToDevice) == cudaSuccess;
     }
+  // working memory of a tick over a full pool, allocated once here instead of during the first
+  // large ticks (one node per particle: the trees of these systems need about half that)
+  ok = ok && serve_reserve(s) == cudaSuccess;
   cudaSetDevice(prev);
   if(!ok)
     {
@@ -443,7 +523,7 @@ int32_t gpugrav_serve_destroy(gpugrav_serve *s)
   for(auto *r : s->finished)
     delete r;
   gg::DevBuf *bufs[] = {&s->pos, &s->vel, &s->acc, &s->oldacc, &s->stype, &s->sysdev, &s->cstart,
-                        &s->c2p, &s->csys, &s->s2p, &s->ntot_dev};
+                        &s->ext, &s->up, &s->dl, &s->c2p, &s->csys, &s->s2p, &s->ntot_dev};
   for(auto *b : bufs)
     b->release();
   s->staging.release();
@@ -474,10 +554,17 @@ int32_t gpugrav_serve_submit(gpugrav_serve *s, int64_t id, int64_t n, const doub
   r->n      = n;
   r->nsteps = nsteps;
   r->dt     = dt;
-  r->pos.assign(pos, pos + 3 * n);
-  r->vel.assign(vel, vel + 3 * n);
-  r->mass.assign(mass, mass + n);
-  r->st.assign(softtype, softtype + n);
+  r->in.reset(new(std::nothrow) double[7 * n]);
+  r->st.reset(new(std::nothrow) uint8_t[n]);
+  if(!r->in || !r->st)
+    {
+      delete r;
+      return sfail(s, GPUGRAV_ERR_OOM, "request copy");
+    }
+  memcpy(r->in.get(), pos, 3 * n * sizeof(double));
+  memcpy(r->in.get() + 3 * n, vel, 3 * n * sizeof(double));
+  memcpy(r->in.get() + 6 * n, mass, n * sizeof(double));
+  memcpy(r->st.get(), softtype, n);
   r->t_submit = now_s();
   s->queue.push_back(r);
   s->stats.submitted++;
@@ -526,6 +613,7 @@ int32_t gpugrav_serve_tick(gpugrav_serve *s, int32_t *n_active)
   const double t_tick = now_s();
 
   // ---- admission (arrival order) ----
+  std::vector<gpugrav_serve::Req *> admitted;
   while(!s->queue.empty() && (int)s->active.size() < s->cfg.max_systems)
     {
       gpugrav_serve::Req *r = s->queue.front();
@@ -539,24 +627,25 @@ int32_t gpugrav_serve_tick(gpugrav_serve *s, int32_t *n_active)
       r->pool_off = off;
       r->state    = ST_NEW;
       r->t_admit  = t_tick;
-      // upload: (x, y, z, m), (vx, vy, vz, 0), softening types
-      size_t need = (size_t)r->n * (2 * sizeof(double4)) + r->n;
-      if(s->staging.ensure(need) != cudaSuccess)
-        return sfail(s, GPUGRAV_ERR_OOM, "staging buffer");
-      double4 *hp = (double4 *)s->staging.p, *hv = hp + r->n;
-      uint8_t *hs = (uint8_t *)(hv + r->n);
-      for(int64_t i = 0; i < r->n; i++)
-        {
-          hp[i] = make_double4(r->pos[3 * i], r->pos[3 * i + 1], r->pos[3 * i + 2], r->mass[i]);
-          hv[i] = make_double4(r->vel[3 * i], r->vel[3 * i + 1], r->vel[3 * i + 2], 0.0);
-          hs[i] = r->st[i];
-        }
-      SCK(cudaMemcpyAsync(s->pos.as<double4>() + off, hp, r->n * sizeof(double4), cudaMemcpyHostToDevice, st), "upload");
-      SCK(cudaMemcpyAsync(s->vel.as<double4>() + off, hv, r->n * sizeof(double4), cudaMemcpyHostToDevice, st), "upload");
-      SCK(cudaMemcpyAsync(s->stype.as<uint8_t>() + off, hs, r->n, cudaMemcpyHostToDevice, st), "upload");
-      SCK(cudaStreamSynchronize(st), "upload");  // staging is reused by the next admission
+      // upload as submitted, interleaved on the device: (x, y, z, m), (vx, vy, vz, 0), softening types
+      if(s->up.ensure((size_t)r->n * (7 * sizeof(double) + 1)) != cudaSuccess)
+        return sfail(s, GPUGRAV_ERR_OOM, "upload buffer");
+      double *din  = s->up.as<double>();
+      uint8_t *dst = (uint8_t *)(din + 7 * r->n);
+      SCK(cudaMemcpyAsync(din, r->in.get(), (size_t)r->n * 7 * sizeof(double), cudaMemcpyHostToDevice, st), "upload");
+      SCK(cudaMemcpyAsync(dst, r->st.get(), r->n, cudaMemcpyHostToDevice, st), "upload");
+      k_srv_unpack<<<grid_for(r->n, 256), 256, 0, st>>>(r->n, off, din, dst, s->pos.as<double4>(), s->vel.as<double4>(),
+                                                        s->stype.as<uint8_t>());
+      SCK(cudaGetLastError(), "upload");
+      admitted.push_back(r);  // the next copy into `up` follows this unpack in stream order
       s->active.push_back(r);
       s->stats.admitted++;
+    }
+  if(!admitted.empty())
+    {
+      SCK(cudaStreamSynchronize(st), "upload");  // host copies of the inputs are no longer needed
+      for(auto *r : admitted)
+        r->in.reset(), r->st.reset();
     }
   const double t_admitted = now_s();
   s->stats.admit_s += t_admitted - t_tick;
@@ -588,6 +677,7 @@ int32_t gpugrav_serve_tick(gpugrav_serve *s, int32_t *n_active)
   // ---- kick + drift, keys, sort, gather ----
   const SysDev *dsys = s->sysdev.as<SysDev>();
   cudaEventRecord(c->ev[12], st);
+  c->mark(nullptr);
   k_srv_expand<<<grid_for(ntot, 256), 256, 0, st>>>(ntot, nsys, dsys, s->cstart.as<int64_t>(), s->c2p.as<int64_t>(),
                                                     s->csys.as<int32_t>());
   k_srv_pre<<<grid_for(ntot, 256), 256, 0, st>>>(ntot, dsys, s->c2p.as<int64_t>(), s->csys.as<int32_t>(), s->pos.as<double4>(),
@@ -600,7 +690,11 @@ int32_t gpugrav_serve_tick(gpugrav_serve *s, int32_t *n_active)
      c->oldacc_s.ensure(ntot * 4) != cudaSuccess || c->acc_s.ensure(ntot * 24) != cudaSuccess ||
      c->pot_s.ensure(ntot * 8) != cudaSuccess || c->nint_s.ensure(ntot * 4) != cudaSuccess)
     return sfail(s, GPUGRAV_ERR_OOM, "tick buffers");
-  k_srv_extent<<<nsys, 256, 0, st>>>(nsys, dsys, s->c2p.as<int64_t>(), s->pos.as<double4>(), c->m_doms.as<gpugrav_domain>());
+  SCK(cudaMemsetAsync(s->ext.p, 0xFF, (size_t)nsys * 6 * 8, st), "extent");
+  SCK(cudaMemset2DAsync(s->ext.as<unsigned long long>() + 3, 6 * 8, 0, 3 * 8, nsys, st), "extent");
+  k_srv_extent<<<dim3(nsys, 32), 256, 0, st>>>(nsys, dsys, s->c2p.as<int64_t>(), s->pos.as<double4>(),
+                                               s->ext.as<unsigned long long>());
+  k_srv_domains<<<grid_for(nsys, 128), 128, 0, st>>>(nsys, s->ext.as<unsigned long long>(), c->m_doms.as<gpugrav_domain>());
   k_srv_keys<<<grid_for(ntot, 256), 256, 0, st>>>(ntot, s->csys.as<int32_t>(), s->c2p.as<int64_t>(), s->pos.as<double4>(),
                                                   c->m_doms.as<gpugrav_domain>(), c->key.as<u128>(), c->idx.as<uint32_t>());
   size_t tb = 0;
@@ -626,7 +720,10 @@ int32_t gpugrav_serve_tick(gpugrav_serve *s, int32_t *n_active)
   c->built      = false;
   c->layout32_valid = false;
   int bstat = 0;
+  c->mark("s1 pre+extent+keys+sort+gather");
+  cudaEventRecord(c->ev[16], st);
   SCK(gg::build_stage(c, &bstat), "build");
+  cudaEventRecord(c->ev[17], st);
   if(bstat != GPUGRAV_OK)
     return sfail(s, bstat, "build failed");
   SCK(gg::layout32_stage(c), "layout");
@@ -671,6 +768,7 @@ int32_t gpugrav_serve_tick(gpugrav_serve *s, int32_t *n_active)
       s->graph_key = key;
       s->graph_captures++;
     }
+  c->mark("s2 walk prepare+capture");
   cudaEventRecord(c->ev[14], st);
   SCK(cudaGraphLaunch(s->graph, st), "walk graph");
   cudaEventRecord(c->ev[15], st);
@@ -681,20 +779,25 @@ int32_t gpugrav_serve_tick(gpugrav_serve *s, int32_t *n_active)
   SCK(cudaMemcpyAsync(&inter, c->counters.as<int>() + 32, 8, cudaMemcpyDeviceToHost, st), "walk flags");
   SCK(cudaMemsetAsync(c->counters.as<int>() + 32, 0, 8, st), "walk flags");
   SCK(cudaStreamSynchronize(st), "tick");
+  c->mark("s3 walk graph");
   if(walk_err)
     return sfail(s, GPUGRAV_ERR_DEEP_TREE, "walk stack exhausted");
 
   // ---- state machine, completion ----
   const double t_end = now_s();
   {
-    float b = 0, w = 0;
+    float b = 0, w = 0, k = 0, t = 0;
     cudaEventElapsedTime(&b, c->ev[12], c->ev[13]);
     cudaEventElapsedTime(&w, c->ev[14], c->ev[15]);
+    cudaEventElapsedTime(&k, c->ev[12], c->ev[16]);
+    cudaEventElapsedTime(&t, c->ev[16], c->ev[17]);
     s->stats.build_s += 1e-3 * b;
+    s->stats.keys_s += 1e-3 * k;
+    s->stats.tree_s += 1e-3 * t;
     s->stats.walk_s += 1e-3 * w;
     s->stats.interactions += (int64_t)inter;
   }
-  std::vector<gpugrav_serve::Req *> keep;
+  std::vector<gpugrav_serve::Req *> keep, done_now;
   for(auto *r : s->active)
     {
       bool done = false;
@@ -716,23 +819,12 @@ int32_t gpugrav_serve_tick(gpugrav_serve *s, int32_t *n_active)
           keep.push_back(r);
           continue;
         }
-      // final state back to the host
-      r->out_pos.resize(3 * r->n);
-      r->out_vel.resize(3 * r->n);
-      r->out_acc.resize(3 * r->n);
-      std::vector<double4> tmp(r->n);
-      SCK(cudaMemcpy(tmp.data(), s->pos.as<double4>() + r->pool_off, r->n * sizeof(double4), cudaMemcpyDeviceToHost), "download");
-      for(int64_t i = 0; i < r->n; i++)
-        r->out_pos[3 * i] = tmp[i].x, r->out_pos[3 * i + 1] = tmp[i].y, r->out_pos[3 * i + 2] = tmp[i].z;
-      SCK(cudaMemcpy(tmp.data(), s->vel.as<double4>() + r->pool_off, r->n * sizeof(double4), cudaMemcpyDeviceToHost), "download");
-      for(int64_t i = 0; i < r->n; i++)
-        r->out_vel[3 * i] = tmp[i].x, r->out_vel[3 * i + 1] = tmp[i].y, r->out_vel[3 * i + 2] = tmp[i].z;
-      SCK(cudaMemcpy(tmp.data(), s->acc.as<double4>() + r->pool_off, r->n * sizeof(double4), cudaMemcpyDeviceToHost), "download");
-      for(int64_t i = 0; i < r->n; i++)
-        r->out_acc[3 * i] = tmp[i].x, r->out_acc[3 * i + 1] = tmp[i].y, r->out_acc[3 * i + 2] = tmp[i].z;
-      pool_free(s, r->pool_off, r->n);
+      done_now.push_back(r);
+    }
+  // finished: results stay in the pool until polled (copied straight into the caller's arrays)
+  for(auto *r : done_now)
+    {
       r->t_done = now_s();
-      r->pos.clear(), r->vel.clear(), r->mass.clear(), r->st.clear();
       s->finished.push_back(r);
       s->stats.completed++;
     }
@@ -763,12 +855,34 @@ int32_t gpugrav_serve_poll(gpugrav_serve *s, int64_t *id, int64_t *n, double *po
   *n                    = r->n;
   if(capacity < r->n)
     return GPUGRAV_OK;  // size reported; call again with room for n particles
-  if(pos)
-    memcpy(pos, r->out_pos.data(), 3 * r->n * sizeof(double));
-  if(vel)
-    memcpy(vel, r->out_vel.data(), 3 * r->n * sizeof(double));
-  if(acc)
-    memcpy(acc, r->out_acc.data(), 3 * r->n * sizeof(double));
+  if(pos || vel || acc)
+    {
+      int prev = 0;
+      cudaGetDevice(&prev);
+      if(prev != s->device)
+        cudaSetDevice(s->device);
+      struct Restore
+      {
+        int d;
+        ~Restore() { cudaSetDevice(d); }
+      } restore{prev};
+      cudaStream_t st = s->st;
+      if(s->dl.ensure((size_t)r->n * 9 * sizeof(double)) != cudaSuccess)
+        return sfail(s, GPUGRAV_ERR_OOM, "download buffer");
+      const double *d = s->dl.as<double>();
+      k_srv_pack<<<grid_for(r->n, 256), 256, 0, st>>>(r->n, r->pool_off, s->pos.as<double4>(), s->vel.as<double4>(),
+                                                      s->acc.as<double4>(), s->dl.as<double>());
+      const size_t b = (size_t)r->n * 3 * sizeof(double);
+      SCK(cudaGetLastError(), "download");
+      if(pos)
+        SCK(cudaMemcpyAsync(pos, d, b, cudaMemcpyDeviceToHost, st), "download");
+      if(vel)
+        SCK(cudaMemcpyAsync(vel, d + 3 * r->n, b, cudaMemcpyDeviceToHost, st), "download");
+      if(acc)
+        SCK(cudaMemcpyAsync(acc, d + 6 * r->n, b, cudaMemcpyDeviceToHost, st), "download");
+      SCK(cudaStreamSynchronize(st), "download");
+    }
+  pool_free(s, r->pool_off, r->n);
   if(times)
     {
       times[0] = r->t_submit;

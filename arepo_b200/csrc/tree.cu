@@ -1020,15 +1020,6 @@ cudaError_t ensure_ph(int device)
 }
 }  // namespace
 
-#define GG_TRY(x)                   \
-  do                                \
-    {                               \
-      cudaError_t _e = (x);         \
-      if(_e != cudaSuccess)         \
-        return _e;                  \
-    }                               \
-  while(0)
-
 cudaError_t toptree_stage(gpugrav_ctx *c, int *status)
 {
   GG_TRY(ensure_ph(c->device));
@@ -1061,6 +1052,58 @@ cudaError_t toptree_stage(gpugrav_ctx *c, int *status)
 }
 
 // Builds the whole tree: skeleton, nodes, moments, threading, walk layout.
+// node arrays for nn nodes
+cudaError_t node_arrays(gpugrav_ctx *c, int64_t nn)
+{
+  cudaError_t e;
+  if((e = c->n_suns.ensure(nn * 8 * sizeof(int32_t))) != cudaSuccess)
+    return e;
+  if((e = c->n_depth.ensure(nn + 16)) != cudaSuccess)
+    return e;
+  if((e = c->n_cl.ensure(nn * sizeof(double4))) != cudaSuccess)
+    return e;
+  if((e = c->n_sm.ensure(nn * sizeof(double4))) != cudaSuccess)
+    return e;
+  if((e = c->n_maxsoft.ensure(nn + 16)) != cudaSuccess)
+    return e;
+  if((e = c->n_size.ensure(nn * sizeof(int32_t))) != cudaSuccess)
+    return e;
+  if((e = c->n_father.ensure(nn * sizeof(int32_t))) != cudaSuccess)
+    return e;
+  if((e = c->n_sibling.ensure(nn * sizeof(int32_t))) != cudaSuccess)
+    return e;
+  if((e = c->n_next.ensure(nn * sizeof(int32_t))) != cudaSuccess)
+    return e;
+  if((e = c->n_dfs.ensure(nn * sizeof(int32_t))) != cudaSuccess)
+    return e;
+  if((e = c->n_first.ensure(nn * sizeof(int32_t))) != cudaSuccess)
+    return e;
+  return cudaSuccess;
+}
+
+// every buffer of build_stage sized for n particles, nn nodes and ntop top nodes (or systems), so
+// that a long-lived caller allocates once
+cudaError_t build_reserve(gpugrav_ctx *c, int64_t n, int64_t nn, int32_t ntop)
+{
+  GG_TRY(c->s_cd.ensure(n + 16));
+  GG_TRY(c->s_tl.ensure(n + 16));
+  GG_TRY(c->s_tlnode.ensure((n + 16) * sizeof(int32_t)));
+  GG_TRY(c->cnt.ensure((n + 16) * sizeof(int32_t)));
+  GG_TRY(c->base.ensure((n + 16) * sizeof(int32_t)));
+  GG_TRY(c->hack_list.ensure((n + 16) * sizeof(int32_t)));
+  GG_TRY(c->counters.ensure(64 * sizeof(int)));
+  GG_TRY(c->skel.ensure(sizeof(SkelInfo) + (size_t)(ntop + 8) * 2 * sizeof(int32_t)));
+  GG_TRY(node_arrays(c, nn + 16));
+  GG_TRY(c->depth_hist.ensure(2 * 256 * sizeof(int)));
+  GG_TRY(c->depth_order.ensure((nn + 16) * sizeof(int32_t)));
+  GG_TRY(c->p_next.ensure((n + 16) * sizeof(int32_t)));
+  GG_TRY(c->p_father.ensure((n + 16) * sizeof(int32_t)));
+  GG_TRY(c->p_dfs.ensure((n + 16) * sizeof(int32_t)));
+  size_t tb = 0;
+  GG_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, c->cnt.as<int32_t>(), c->base.as<int32_t>(), (int)(n + 1), c->stream));
+  return c->sort_tmp.ensure(tb);
+}
+
 cudaError_t build_stage(gpugrav_ctx *c, int *status)
 {
   GG_TRY(ensure_ph(c->device));
@@ -1069,6 +1112,7 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
   cudaStream_t st    = c->stream;
   int launches       = 0;
   *status            = GPUGRAV_OK;
+  c->mark(nullptr);
 
   GG_TRY(c->s_cd.ensure(n + 16));
   GG_TRY(c->s_tl.ensure(n + 16));
@@ -1084,32 +1128,7 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
   int32_t *nodetop  = leafnode + ntop + 4;
 
   // skeleton needs node storage for the first ntop nodes; size node arrays for ntop now, grow later
-  auto ensure_nodes = [&](int64_t nn) -> cudaError_t {
-    cudaError_t e;
-    if((e = c->n_suns.ensure(nn * 8 * sizeof(int32_t))) != cudaSuccess)
-      return e;
-    if((e = c->n_depth.ensure(nn + 16)) != cudaSuccess)
-      return e;
-    if((e = c->n_cl.ensure(nn * sizeof(double4))) != cudaSuccess)
-      return e;
-    if((e = c->n_sm.ensure(nn * sizeof(double4))) != cudaSuccess)
-      return e;
-    if((e = c->n_maxsoft.ensure(nn + 16)) != cudaSuccess)
-      return e;
-    if((e = c->n_size.ensure(nn * sizeof(int32_t))) != cudaSuccess)
-      return e;
-    if((e = c->n_father.ensure(nn * sizeof(int32_t))) != cudaSuccess)
-      return e;
-    if((e = c->n_sibling.ensure(nn * sizeof(int32_t))) != cudaSuccess)
-      return e;
-    if((e = c->n_next.ensure(nn * sizeof(int32_t))) != cudaSuccess)
-      return e;
-    if((e = c->n_dfs.ensure(nn * sizeof(int32_t))) != cudaSuccess)
-      return e;
-    if((e = c->n_first.ensure(nn * sizeof(int32_t))) != cudaSuccess)
-      return e;
-    return cudaSuccess;
-  };
+  auto ensure_nodes = [&](int64_t nn) { return node_arrays(c, nn); };
 
   // 1. per-particle top leaf, pair depths (skeleton first: it validates the top tree and maps leaves to nodes)
   const int32_t *msys            = c->multi ? c->m_sys.as<int32_t>() : nullptr;
@@ -1165,6 +1184,7 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
   a.nn     = 0;
   a.err    = counters + 12;
 
+  c->mark("b1 roots+pairdepth");
   // 2. node counts per inserting particle, replayed cells
   GG_TRY(cudaMemsetAsync(counters, 0, 16 * sizeof(int), st));
   k_count<<<grid_for(n + 1, 256), 256, 0, st>>>(a, c->cnt.as<int32_t>(), c->hack_list.as<int32_t>(), counters);
@@ -1196,6 +1216,7 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
       launches += 2;
     }
 
+  c->mark("b2 count+hack");
   // 3. numbering: exclusive scan of per-particle node counts
   {
     size_t tb = 0;
@@ -1217,6 +1238,7 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
   c->n_entries = n + nn;
   a.nn         = nn;
 
+  c->mark("b3 scan");
   // grow node arrays, keeping the skeleton written by k_skeleton
   if((size_t)nn * 8 * sizeof(int32_t) > c->n_suns.cap || (size_t)nn * sizeof(double4) > c->n_cl.cap ||
      (size_t)nn + 16 > c->n_depth.cap)
@@ -1236,6 +1258,7 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
       launches++;
     }
 
+  c->mark("b3b grow");
   // 4. fill canonical nodes, link, place particles, replay coincident cells
   k_nodes<<<grid_for(n, 256), 256, 0, st>>>(a, c->n_suns.as<int32_t>(), c->n_cl.as<double4>(), c->n_depth.as<uint8_t>(),
                                              c->n_first.as<int32_t>());
@@ -1250,6 +1273,7 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
     }
   GG_TRY(cudaGetLastError());
 
+  c->mark("b4 nodes+link+leaves");
   // 5. depth buckets
   GG_TRY(c->depth_hist.ensure(2 * 256 * sizeof(int)));
   GG_TRY(c->depth_order.ensure((nn + 16) * sizeof(int32_t)));
@@ -1274,6 +1298,7 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
   k_depth_scatter<<<grid_for(nn, 256), 256, 0, st>>>(c->n_depth.as<uint8_t>(), nn, cursor, c->depth_order.as<int32_t>());
   launches += 2;
 
+  c->mark("b5 depth buckets");
   // 6. moments bottom-up
   const int32_t *order = c->depth_order.as<int32_t>();
   for(int d = maxd; d >= 0; d--)
@@ -1287,6 +1312,7 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
                                                    c->bconst.as<BuildConst>());
       launches++;
     }
+  c->mark("b6 moments");
   // 7. threading top-down
   GG_TRY(c->p_next.ensure((n + 16) * sizeof(int32_t)));
   GG_TRY(c->p_father.ensure((n + 16) * sizeof(int32_t)));
@@ -1314,16 +1340,21 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
                                                c->p_father.as<int32_t>());
       launches++;
     }
-  // 8. walk layout
-  const int64_t ne = n + nn;
-  GG_TRY(c->w_sm.ensure(ne * sizeof(double4)));
-  GG_TRY(c->w_cl.ensure(ne * sizeof(double4)));
-  GG_TRY(c->w_link.ensure(ne * sizeof(int2)));
-  k_layout<<<grid_for(ne, 256), 256, 0, st>>>(n, nn, c->s_pm.as<double4>(), c->s_st.as<uint8_t>(), c->p_dfs.as<int32_t>(),
-                                               c->n_sm.as<double4>(), c->n_cl.as<double4>(), c->n_maxsoft.as<uint8_t>(),
-                                               c->n_size.as<int32_t>(), c->n_dfs.as<int32_t>(), c->w_sm.as<double4>(),
-                                               c->w_cl.as<double4>(), c->w_link.as<int2>(), a.err);
-  launches++;
+  c->mark("b7 threading");
+  // 8. walk layout of the FP64 walk (several systems are walked by the FP32 group walk only)
+  if(!c->multi)
+    {
+      const int64_t ne = n + nn;
+      GG_TRY(c->w_sm.ensure(ne * sizeof(double4)));
+      GG_TRY(c->w_cl.ensure(ne * sizeof(double4)));
+      GG_TRY(c->w_link.ensure(ne * sizeof(int2)));
+      k_layout<<<grid_for(ne, 256), 256, 0, st>>>(n, nn, c->s_pm.as<double4>(), c->s_st.as<uint8_t>(), c->p_dfs.as<int32_t>(),
+                                                   c->n_sm.as<double4>(), c->n_cl.as<double4>(), c->n_maxsoft.as<uint8_t>(),
+                                                   c->n_size.as<int32_t>(), c->n_dfs.as<int32_t>(), c->w_sm.as<double4>(),
+                                                   c->w_cl.as<double4>(), c->w_link.as<int2>(), a.err);
+      launches++;
+    }
+  c->mark("b8 layout64");
   c->timings.build_kernel_launches = launches;
   GG_TRY(cudaGetLastError());
   int err = 0;

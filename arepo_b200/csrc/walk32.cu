@@ -771,14 +771,44 @@ void make_w32(const WalkConst &wc, W32Const *w)
 }
 }  // namespace
 
-#define GG_TRY(x)             \
-  do                          \
-    {                         \
-      cudaError_t _e = (x);   \
-      if(_e != cudaSuccess)   \
-        return _e;            \
-    }                         \
-  while(0)
+// buffers of the FP32 walk layout and group table for n particles and nn nodes
+cudaError_t layout32_buffers(gpugrav_ctx *c, int64_t n, int64_t nn)
+{
+  GG_TRY(c->g_key.ensure(nn * 8));
+  GG_TRY(c->g_key_alt.ensure(nn * 8));
+  GG_TRY(c->g_val.ensure(nn * 4));
+  GG_TRY(c->g_val_alt.ensure(nn * 4));
+  GG_TRY(c->g_bfs.ensure(nn * 4));
+  GG_TRY(c->g_np.ensure((nn + 1) * 4));
+  GG_TRY(c->g_poff.ensure((nn + 1) * 4));
+  GG_TRY(c->g_sm.ensure(nn * sizeof(double4)));
+  GG_TRY(c->g_rel.ensure(nn * sizeof(float4)));
+  GG_TRY(c->g_kids.ensure(nn * sizeof(int4)));
+  GG_TRY(c->g_pm.ensure(n * sizeof(double4)));
+  GG_TRY(c->g_pst.ensure(n + 16));
+  GG_TRY(c->g_groups.ensure(n * sizeof(int4)));
+  GG_TRY(c->g_ngroups.ensure(16));
+  GG_TRY(c->g_gpd.ensure(n + 16));
+  GG_TRY(c->g_gseg.ensure(n * 4));
+  GG_TRY(c->g_gflag.ensure(n * 4));
+  GG_TRY(c->g_gid.ensure(n * 4));
+  return cudaSuccess;
+}
+
+// layout32_stage's buffers and temporary storage sized once for n particles and nn nodes
+cudaError_t layout32_reserve(gpugrav_ctx *c, int64_t n, int64_t nn)
+{
+  GG_TRY(layout32_buffers(c, n, nn));
+  size_t tb = 0, t2 = 0;
+  GG_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, c->g_key.as<uint64_t>(), c->g_key_alt.as<uint64_t>(),
+                                         c->g_val.as<int32_t>(), c->g_val_alt.as<int32_t>(), (int)nn, 0, 40, c->stream));
+  GG_TRY(cub::DeviceScan::InclusiveScan(nullptr, t2, c->g_gflag.as<int32_t>(), c->g_gseg.as<int32_t>(), MaxOp32(), (int)n,
+                                        c->stream));
+  tb = t2 > tb ? t2 : tb;
+  GG_TRY(cub::DeviceScan::ExclusiveSum(nullptr, t2, c->g_gflag.as<int32_t>(), c->g_gid.as<int32_t>(), (int)n, c->stream));
+  tb = t2 > tb ? t2 : tb;
+  return c->sort_tmp.ensure(tb);
+}
 
 // walk group table of the current tree (see k_grp_pd); the group count stays on the device
 cudaError_t groups_stage(gpugrav_ctx *c)
@@ -786,12 +816,6 @@ cudaError_t groups_stage(gpugrav_ctx *c)
   const int64_t n = c->n;
   cudaStream_t st = c->stream;
   const int cap   = 32 * ((c->walk32_tpl == 1 || c->multi) ? 1 : 2);
-  GG_TRY(c->g_groups.ensure(n * sizeof(int4)));
-  GG_TRY(c->g_ngroups.ensure(16));
-  GG_TRY(c->g_gpd.ensure(n + 16));
-  GG_TRY(c->g_gseg.ensure(n * 4));
-  GG_TRY(c->g_gflag.ensure(n * 4));
-  GG_TRY(c->g_gid.ensure(n * 4));
   GG_TRY(cudaMemsetAsync(c->g_ngroups.p, 0, sizeof(int), st));
   if(n == 0)
     return cudaSuccess;
@@ -819,20 +843,10 @@ cudaError_t groups_stage(gpugrav_ctx *c)
 // breadth-first node layout + particles grouped by parent (built once per tree)
 cudaError_t layout32_stage(gpugrav_ctx *c)
 {
+  c->mark(nullptr);
   const int64_t n = c->n, nn = c->num_nodes;
   cudaStream_t st = c->stream;
-  GG_TRY(c->g_key.ensure(nn * 8));
-  GG_TRY(c->g_key_alt.ensure(nn * 8));
-  GG_TRY(c->g_val.ensure(nn * 4));
-  GG_TRY(c->g_val_alt.ensure(nn * 4));
-  GG_TRY(c->g_bfs.ensure(nn * 4));
-  GG_TRY(c->g_np.ensure((nn + 1) * 4));
-  GG_TRY(c->g_poff.ensure((nn + 1) * 4));
-  GG_TRY(c->g_sm.ensure(nn * sizeof(double4)));
-  GG_TRY(c->g_rel.ensure(nn * sizeof(float4)));
-  GG_TRY(c->g_kids.ensure(nn * sizeof(int4)));
-  GG_TRY(c->g_pm.ensure(n * sizeof(double4)));
-  GG_TRY(c->g_pst.ensure(n + 16));
+  GG_TRY(layout32_buffers(c, n, nn));
   k_g_keys<<<grid_for(nn, 256), 256, 0, st>>>(nn, c->n_depth.as<uint8_t>(), c->n_dfs.as<int32_t>(), c->g_key.as<uint64_t>(),
                                                c->g_val.as<int32_t>());
   size_t tb = 0;
@@ -860,7 +874,9 @@ cudaError_t layout32_stage(gpugrav_ctx *c)
   GG_TRY(cudaStreamSynchronize(st));
   if(e)
     return cudaErrorUnknown;
+  c->mark("l1 layout32");
   GG_TRY(groups_stage(c));
+  c->mark("l2 groups");
   c->layout32_valid = true;
   return cudaSuccess;
 }

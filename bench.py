@@ -259,13 +259,16 @@ def run_stream(systems, ids, arrivals, max_systems, device, max_particles):
         s0 = srv.stats()
         arrive, lat, svc, sizes = {}, [], [], []
         k, nsys_ticks = 0, 0
+        t_sub = t_poll = 0.0
         t0 = time.monotonic()
         while True:
             now = time.monotonic() - t0
             while k < len(ids) and (arrivals is None or arrivals[k] <= now):
                 i = int(ids[k])
                 arrive[i] = t0 + (0.0 if arrivals is None else float(arrivals[k]))
+                ts = time.monotonic()
                 srv.submit(i, *systems[i], nsteps=SERVE_K, dt=SERVE_DT)
+                t_sub += time.monotonic() - ts
                 k += 1
             if not srv.busy():
                 if k >= len(ids):
@@ -274,10 +277,12 @@ def run_stream(systems, ids, arrivals, max_systems, device, max_particles):
                 continue
             srv.tick()
             nsys_ticks += srv.stats().last_tick_systems
+            tp = time.monotonic()
             for r in srv.poll_all():
                 lat.append(time.monotonic() - arrive[r.id])
                 svc.append(r.t_done - r.t_admit)
                 sizes.append(len(r.pos))
+            t_poll += time.monotonic() - tp
         wall = time.monotonic() - t0
         s1 = srv.stats()
     ticks = s1.ticks - s0.ticks
@@ -286,7 +291,9 @@ def run_stream(systems, ids, arrivals, max_systems, device, max_particles):
             "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
             "service_p50_s": float(np.percentile(svc, 50)), "service_p99_s": float(np.percentile(svc, 99)),
             "ticks": int(ticks), "mean_systems_per_tick": nsys_ticks / max(ticks, 1),
-            "phase_s": {k: getattr(s1, k) - getattr(s0, k) for k in ("admit_s", "build_s", "walk_s", "finish_s")},
+            "phase_s": dict({k: getattr(s1, k) - getattr(s0, k)
+                             for k in ("admit_s", "build_s", "keys_s", "tree_s", "walk_s", "finish_s")},
+                            submit_s=t_sub, poll_s=t_poll),
             "interactions_per_particle_step": (s1.interactions - s0.interactions) / max(1, s1.particle_steps - s0.particle_steps),
             "graph_captures": int(s1.graph_captures - s0.graph_captures),
             "graph_replays": int(s1.graph_replays - s0.graph_replays)}

@@ -244,6 +244,7 @@ typedef struct gpugrav_serve_stats
    * walk + store/kick (device), completion (downloads + unpacking) */
   double admit_s, build_s, walk_s, finish_s;
   int64_t interactions;  /* particle-node and particle-particle interactions of all walks */
+  double keys_s, tree_s; /* parts of build_s: kick/drift + keys + sort + gather; octree build */
 } gpugrav_serve_stats;
 
 int32_t gpugrav_serve_create(gpugrav_serve **srv, int32_t device, const gpugrav_params *params,
@@ -257,7 +258,9 @@ int32_t gpugrav_serve_cancel(gpugrav_serve *srv, int64_t id);
 /* one force evaluation for every admitted system (admission first); n_active may be NULL */
 int32_t gpugrav_serve_tick(gpugrav_serve *srv, int32_t *n_active);
 /* oldest finished request: *id = -1 when none. With capacity < *n only id and n are returned and the
- * result stays queued. times (may be NULL): submit, admit, done (seconds, steady clock). */
+ * result stays queued. times (may be NULL): submit, admit, done (seconds, steady clock).
+ * A finished request keeps its particles on the device (counted against the memory budget) until
+ * it is polled; pos, vel, acc (host, n*3 each, any may be NULL) are then copied from the device. */
 int32_t gpugrav_serve_poll(gpugrav_serve *srv, int64_t *id, int64_t *n, double *pos, double *vel, double *acc,
                            int64_t capacity, double *times);
 int32_t gpugrav_serve_get_stats(gpugrav_serve *srv, gpugrav_serve_stats *stats);
