@@ -310,8 +310,9 @@ struct gpugrav_serve
     int64_t n  = 0;
     int32_t nsteps = 0;
     double dt      = 0;
-    std::unique_ptr<double[]> in;  // pos (3n) | vel (3n) | mass (n), until admitted
+    std::unique_ptr<double[]> in;  // pos (3n) | vel (3n) | mass (n), until admitted (not resident)
     std::unique_ptr<uint8_t[]> st;
+    bool resident = false;         // particles already in the pool (placed at submission)
     // running
     int32_t state = ST_NEW, steps_done = 0;
     int64_t pool_off = -1;
@@ -423,6 +424,23 @@ cudaError_t serve_reserve(gpugrav_serve *s)
   GG_TRY(gg::layout32_reserve(c, n, n));
   GG_TRY(s->up.ensure((size_t)n * (7 * sizeof(double) + 1)));
   return s->dl.ensure((size_t)n * 9 * sizeof(double));
+}
+
+// caller arrays -> pool at off, through the upload buffer: (x, y, z, m), (vx, vy, vz, 0), types
+cudaError_t upload(gpugrav_serve *s, int64_t off, int64_t n, const double *pos, const double *vel, const double *mass,
+                   const uint8_t *st)
+{
+  cudaStream_t q = s->st;
+  GG_TRY(s->up.ensure((size_t)n * (7 * sizeof(double) + 1)));
+  double *din  = s->up.as<double>();
+  uint8_t *dst = (uint8_t *)(din + 7 * n);
+  GG_TRY(cudaMemcpyAsync(din, pos, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice, q));
+  GG_TRY(cudaMemcpyAsync(din + 3 * n, vel, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice, q));
+  GG_TRY(cudaMemcpyAsync(din + 6 * n, mass, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, q));
+  GG_TRY(cudaMemcpyAsync(dst, st, n, cudaMemcpyHostToDevice, q));
+  k_srv_unpack<<<grid_for(n, 256), 256, 0, q>>>(n, off, din, dst, s->pos.as<double4>(), s->vel.as<double4>(),
+                                                s->stype.as<uint8_t>());
+  return cudaGetLastError();
 }
 
 int64_t in_flight(const gpugrav_serve *s)
@@ -554,17 +572,46 @@ int32_t gpugrav_serve_submit(gpugrav_serve *s, int64_t id, int64_t n, const doub
   r->n      = n;
   r->nsteps = nsteps;
   r->dt     = dt;
-  r->in.reset(new(std::nothrow) double[7 * n]);
-  r->st.reset(new(std::nothrow) uint8_t[n]);
-  if(!r->in || !r->st)
+  // Straight into the pool when it has room and everything queued is resident too (pool ranges
+  // then follow the admission order, so a resident request never holds memory that a request
+  // ahead of it waits for); otherwise a host copy, uploaded at admission.
+  bool all_resident = true;
+  for(auto *q : s->queue)
+    all_resident = all_resident && q->resident;
+  int64_t off = -1;
+  if(all_resident && pool_alloc(s, n, &off))
     {
-      delete r;
-      return sfail(s, GPUGRAV_ERR_OOM, "request copy");
+      int prev = 0;
+      cudaGetDevice(&prev);
+      if(prev != s->device)
+        cudaSetDevice(s->device);
+      cudaError_t e = upload(s, off, n, pos, vel, mass, softtype);
+      if(e == cudaSuccess)
+        e = cudaStreamSynchronize(s->st);  // the caller's arrays may change after return
+      cudaSetDevice(prev);
+      if(e != cudaSuccess)
+        {
+          pool_free(s, off, n);
+          delete r;
+          return sfail(s, GPUGRAV_ERR_CUDA, "upload", e);
+        }
+      r->resident = true;
+      r->pool_off = off;
     }
-  memcpy(r->in.get(), pos, 3 * n * sizeof(double));
-  memcpy(r->in.get() + 3 * n, vel, 3 * n * sizeof(double));
-  memcpy(r->in.get() + 6 * n, mass, n * sizeof(double));
-  memcpy(r->st.get(), softtype, n);
+  else
+    {
+      r->in.reset(new(std::nothrow) double[7 * n]);
+      r->st.reset(new(std::nothrow) uint8_t[n]);
+      if(!r->in || !r->st)
+        {
+          delete r;
+          return sfail(s, GPUGRAV_ERR_OOM, "request copy");
+        }
+      memcpy(r->in.get(), pos, 3 * n * sizeof(double));
+      memcpy(r->in.get() + 3 * n, vel, 3 * n * sizeof(double));
+      memcpy(r->in.get() + 6 * n, mass, n * sizeof(double));
+      memcpy(r->st.get(), softtype, n);
+    }
   r->t_submit = now_s();
   s->queue.push_back(r);
   s->stats.submitted++;
@@ -578,6 +625,8 @@ int32_t gpugrav_serve_cancel(gpugrav_serve *s, int64_t id)
   for(auto it = s->queue.begin(); it != s->queue.end(); ++it)
     if((*it)->id == id)
       {
+        if((*it)->resident)
+          pool_free(s, (*it)->pool_off, (*it)->n);
         delete *it;
         s->queue.erase(it);
         s->stats.cancelled++;
@@ -620,24 +669,19 @@ int32_t gpugrav_serve_tick(gpugrav_serve *s, int32_t *n_active)
       int64_t fl            = in_flight(s);
       if(s->cfg.memory_budget_bytes > 0 && (fl + r->n) * s->bytes_per_particle > s->cfg.memory_budget_bytes)
         break;
-      int64_t off;
-      if(!pool_alloc(s, r->n, &off))
-        break;
+      if(!r->resident)
+        {
+          int64_t off;
+          if(!pool_alloc(s, r->n, &off))
+            break;
+          r->pool_off = off;
+          const double *in = r->in.get();
+          SCK(upload(s, off, r->n, in, in + 3 * r->n, in + 6 * r->n, r->st.get()), "upload");
+          admitted.push_back(r);  // the next copy into `up` follows this unpack in stream order
+        }
       s->queue.pop_front();
-      r->pool_off = off;
-      r->state    = ST_NEW;
-      r->t_admit  = t_tick;
-      // upload as submitted, interleaved on the device: (x, y, z, m), (vx, vy, vz, 0), softening types
-      if(s->up.ensure((size_t)r->n * (7 * sizeof(double) + 1)) != cudaSuccess)
-        return sfail(s, GPUGRAV_ERR_OOM, "upload buffer");
-      double *din  = s->up.as<double>();
-      uint8_t *dst = (uint8_t *)(din + 7 * r->n);
-      SCK(cudaMemcpyAsync(din, r->in.get(), (size_t)r->n * 7 * sizeof(double), cudaMemcpyHostToDevice, st), "upload");
-      SCK(cudaMemcpyAsync(dst, r->st.get(), r->n, cudaMemcpyHostToDevice, st), "upload");
-      k_srv_unpack<<<grid_for(r->n, 256), 256, 0, st>>>(r->n, off, din, dst, s->pos.as<double4>(), s->vel.as<double4>(),
-                                                        s->stype.as<uint8_t>());
-      SCK(cudaGetLastError(), "upload");
-      admitted.push_back(r);  // the next copy into `up` follows this unpack in stream order
+      r->state   = ST_NEW;
+      r->t_admit = t_tick;
       s->active.push_back(r);
       s->stats.admitted++;
     }

@@ -299,6 +299,56 @@ def run_stream(systems, ids, arrivals, max_systems, device, max_particles):
             "graph_replays": int(s1.graph_replays - s0.graph_replays)}
 
 
+def run_plain_serial(systems, ids, device):
+    """The same requests one at a time through the plain per-call API: one gpugrav_compute per force
+    evaluation on host arrays (upload, keys, sort, build, walk, download), kick and drift on the host
+    -- the pattern of a code that calls gravity once per step."""
+    from arepo_b200 import _lib as L
+    from arepo_b200.gravity import GravityTree
+    from arepo_b200.serving import serving_params
+
+    prm = serving_params(SERVE_EPS)
+    theta = prm.err_tol_theta
+    lat, steps = [], 0
+    with GravityTree(prm, device=device) as t:
+        lib, ctx = t.lib, t._ctx
+
+        def force(x, mass, st, old):
+            n = len(mass)
+            acc = np.empty((n, 3))
+            ni = np.empty(n, np.int32)
+            s = lib.gpugrav_compute(ctx, n, L.ptr(x), L.ptr(mass), L.ptr(st), None if old is None else L.ptr(old), None,
+                                    None, 0, L.ptr(acc), None, L.ptr(ni), L.MEM_HOST)
+            if s != 0:
+                raise L.GpuGravError(s, lib.gpugrav_last_error(ctx).decode())
+            return acc
+
+        def run(i):
+            pos, vel, mass, st = systems[i]
+            x, v = pos.copy(), vel.copy()
+            prm.err_tol_theta = theta
+            t.set_params(prm)
+            a = force(x, mass, st, None)  # Barnes-Hut pass
+            prm.err_tol_theta = 0.0
+            t.set_params(prm)
+            a = force(x, mass, st, np.linalg.norm(a, axis=1).astype(np.float32))  # relative pass
+            for _ in range(SERVE_K):
+                v += 0.5 * SERVE_DT * a
+                x += SERVE_DT * v
+                a = force(x, mass, st, np.linalg.norm(a, axis=1).astype(np.float32))
+                v += 0.5 * SERVE_DT * a
+            return (SERVE_K + 2) * len(mass)
+
+        run(int(ids[0]))  # warm-up
+        t0 = time.monotonic()
+        for i in ids:
+            steps += run(int(i))
+            lat.append(time.monotonic() - t0)
+        wall = time.monotonic() - t0
+    return {"requests": len(ids), "wall_s": wall, "requests_per_s": len(ids) / wall, "particle_steps_per_s": steps / wall,
+            "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99))}
+
+
 def serving_leg(args, device):
     ns, kinds = serving_stream(args.serve_requests)
     t = time.time()
@@ -311,6 +361,8 @@ def serving_leg(args, device):
     log(f"serving: batched {batched['requests_per_s']:.2f} req/s")
     serial = run_stream(systems, cmp_ids, None, 1, device, pool)
     log(f"serving: serial {serial['requests_per_s']:.2f} req/s")
+    plain = run_plain_serial(systems, cmp_ids, device)
+    log(f"serving: plain API serial {plain['requests_per_s']:.2f} req/s")
     rate = args.serve_load * batched["requests_per_s"]
     arr = np.cumsum(np.random.default_rng(1006).exponential(1.0 / rate, len(ns)))
     poisson = run_stream(systems, np.arange(len(ns)), arr, 4096, device, pool)
@@ -321,8 +373,13 @@ def serving_leg(args, device):
                   f"BH pass + relative pass (ErrTolForceAcc 0.0025) + K={SERVE_K} KDK steps of dt={SERVE_DT}, "
                   f"FP32 walk, {SERVE_BUDGET / 1e9:.0f} GB admission budget",
         "particles": int(ns.sum()),
-        "compare": {"requests": int(ncmp), "arrivals": "all at t=0", "batched": batched, "serial_max_systems_1": serial,
-                    "throughput_ratio": batched["particle_steps_per_s"] / serial["particle_steps_per_s"]},
+        "compare": {"requests": int(ncmp), "arrivals": "all at t=0", "batched": batched,
+                    "serial_max_systems_1": serial, "serial_plain_api": plain,
+                    "throughput_ratio": batched["particle_steps_per_s"] / serial["particle_steps_per_s"],
+                    "throughput_ratio_vs_plain_api": batched["particle_steps_per_s"] / plain["particle_steps_per_s"],
+                    "serial_note": "serial_max_systems_1: the serving loop admitting one request at a time (device-"
+                                   "resident particles, the same kernels); serial_plain_api: one gpugrav_compute call "
+                                   "per force evaluation on host arrays, kick/drift on the host"},
         "poisson": dict(poisson, rate_per_s=rate, load=args.serve_load),
         "clock": "host wall clock of the serving loop (uploads, ticks, downloads included)",
     }
