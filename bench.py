@@ -55,6 +55,10 @@ sys.path.insert(0, ROOT)
 METRIC = "tree-gravity particles/s at N=2^24 (RMS force err ≤1e-3); serving p50/p99 latency"
 UNIT = "particles/s"
 FLOPS_PER_INTERACTION = 23.0  # convention of the path's roofline
+# DRAM bytes (read + write) of one FP32 walk launch per particle: ncu capture of the zoom box at
+# N=2^21 (dram__bytes_read.sum + dram__bytes_write.sum = 299 MB + 90 MB), scaled by the particle
+# count (the walk reads the tree and the particles once from DRAM; everything else hits in L2)
+WALK32_DRAM_BYTES_PER_PARTICLE = 388.8e6 / (1 << 21)
 
 
 def log(*a):
@@ -531,7 +535,9 @@ def our_arm(args):
     ia = float(np.mean(inter))
     achieved = FLOPS_PER_INTERACTION * ia / walk_s / 1e12
     roofline = {"bound": "fp32" if prec == L.PREC_FP32 else "fp64", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak if peak > 0 else None, "traffic": None,
+                "unit": "TFLOP/s", "frac": achieved / peak if peak > 0 else None,
+                "traffic": WALK32_DRAM_BYTES_PER_PARTICLE * n if prec == L.PREC_FP32 else None,
+                "traffic_source": "ncu capture of the N=2^21 zoom box walk scaled by particle count",
                 "kernel": "k_walk32" if prec == L.PREC_FP32 else "k_walk64",
                 "peak_source": "measured in-run: CUDA-core FMA microbenchmark (gpugrav_measure_fma_peak); "
                                "MEASURED_PEAKS.json has no CUDA-core figure",
