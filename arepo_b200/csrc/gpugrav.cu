@@ -504,6 +504,17 @@ int32_t gpugrav_build(gpugrav_ctx *c, const gpugrav_topnode *top, int32_t ntop)
   return GPUGRAV_OK;
 }
 
+int32_t gpugrav_set_target_slice(gpugrav_ctx *c, int32_t slice, int32_t nslices)
+{
+  if(!c)
+    return GPUGRAV_ERR_INVALID;
+  if(nslices < 1 || slice < 0 || slice >= nslices)
+    return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_set_target_slice: need 0 <= slice < nslices");
+  c->slice   = slice;
+  c->nslices = nslices;
+  return GPUGRAV_OK;
+}
+
 int32_t gpugrav_walk(gpugrav_ctx *c, const float *oldacc, double *acc, double *pot, int32_t *ninter, int32_t mem)
 {
   if(!c)
@@ -547,6 +558,7 @@ int32_t gpugrav_walk(gpugrav_ctx *c, const float *oldacc, double *acc, double *p
     {
       CK(gg::walk64_stage(c, wc), "fp64 walk");
     }
+  CK(gg::slice_mask_stage(c, c->prm.precision == GPUGRAV_PREC_FP32), "target slice");
   cudaEventRecord(c->ev[9], st);
   double *d_acc = acc, *d_pot = pot;
   int32_t *d_nint = ninter;

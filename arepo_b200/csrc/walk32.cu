@@ -346,6 +346,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                                                         const uint8_t *__restrict__ g_pst, const double4 *__restrict__ tpm,
                                                         const uint8_t *__restrict__ tst, const float *__restrict__ oldacc,
                                                         const int *__restrict__ ngroups_dev, const int4 *__restrict__ groups,
+                                                        int slice, int nslices,
                                                         const W32Const *__restrict__ wcp,
                                                         int *__restrict__ stack_base, int *__restrict__ work,
                                                         double *__restrict__ acc_out, double *__restrict__ pot_out,
@@ -366,15 +367,17 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
   float4 *LP             = il_p[warp];
   float *LH              = il_h[warp];
   unsigned long long my_total = 0;
-  const int ng           = *ngroups_dev;  // device-side count: no host round trip, graph replays
+  // groups of this target slice; the count lives on the device (no host round trip, graph replays)
+  const int64_t ng       = *ngroups_dev;
+  const int g_begin      = (int)(ng * slice / nslices), g_end = (int)(ng * (slice + 1) / nslices);
 
   while(true)
     {
       int grp = 0;
       if(lane == 0)
         grp = atomicAdd(work, 1);
-      grp = __shfl_sync(0xffffffffu, grp, 0);
-      if(grp >= ng)
+      grp = g_begin + __shfl_sync(0xffffffffu, grp, 0);
+      if(grp >= g_end)
         break;
       // group of up to 32*TPL consecutive targets; lane holds targets t0 + lane + 32k.  A group lies
       // inside one system and walks that system's tree (root).
@@ -733,6 +736,34 @@ __global__ void k_grp_fill(int64_t n, const int32_t *__restrict__ flag, const in
     }
 }
 
+// outputs (sorted order) of the targets outside this slice set to zero; the slice's target range
+// is [start of group g_begin, start of group g_end) with the FP32 group table, else n*s/ns..
+__global__ void k_slice_mask(int64_t n, int slice, int nslices, const int4 *__restrict__ groups, const int *__restrict__ ngroups,
+                             double *__restrict__ acc, double *__restrict__ pot, int32_t *__restrict__ nint)
+{
+  int64_t t_begin, t_end;
+  if(groups)
+    {
+      const int64_t ng = *ngroups;
+      const int64_t gb = ng * slice / nslices, ge = ng * (slice + 1) / nslices;
+      t_begin          = gb < ng ? groups[gb].x : n;
+      t_end            = ge < ng ? groups[ge].x : n;
+    }
+  else
+    {
+      t_begin = n * slice / nslices;
+      t_end   = n * (slice + 1) / nslices;
+    }
+  for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if(i < t_begin || i >= t_end)
+      {
+        acc[3 * i] = acc[3 * i + 1] = acc[3 * i + 2] = 0.0;
+        if(pot)
+          pot[i] = 0.0;
+        nint[i] = 0;
+      }
+}
+
 struct MaxOp32
 {
   __device__ __forceinline__ int32_t operator()(int32_t a, int32_t b) const { return a > b ? a : b; }
@@ -926,9 +957,20 @@ cudaError_t walk32_launch(gpugrav_ctx *c)
   kern<<<c->w32_blocks, 32 * kWarps, 0, st>>>(c->g_sm.as<double4>(), c->g_rel.as<float4>(), c->g_kids.as<int4>(),
                                               c->g_pm.as<double4>(), c->g_pst.as<uint8_t>(), c->s_pm.as<double4>(),
                                               c->s_st.as<uint8_t>(), c->oldacc_s.as<float>(), c->g_ngroups.as<int>(),
-                                              c->g_groups.as<int4>(), (const W32Const *)c->scratch.p,
+                                              c->g_groups.as<int4>(), c->slice, c->nslices, (const W32Const *)c->scratch.p,
                                               c->g_stack.as<int>(), work, c->acc_s.as<double>(), c->pot_s.as<double>(),
                                               c->nint_s.as<int32_t>(), (unsigned long long *)(c->counters.as<int>() + 32), err);
+  return cudaGetLastError();
+}
+
+// zero the outputs of the targets outside the current target slice (no-op without slicing)
+cudaError_t slice_mask_stage(gpugrav_ctx *c, bool fp32)
+{
+  if(c->nslices <= 1)
+    return cudaSuccess;
+  k_slice_mask<<<grid_for(c->n, 256), 256, 0, c->stream>>>(c->n, c->slice, c->nslices, fp32 ? c->g_groups.as<int4>() : nullptr,
+                                                           fp32 ? c->g_ngroups.as<int>() : nullptr, c->acc_s.as<double>(),
+                                                           c->want_pot ? c->pot_s.as<double>() : nullptr, c->nint_s.as<int32_t>());
   return cudaGetLastError();
 }
 

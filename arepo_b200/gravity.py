@@ -59,6 +59,11 @@ class GravityTree:
         self._check(self.lib.gpugrav_set_params(self._ctx, C.byref(params)))
         self.params = params
 
+    def set_target_slice(self, slice_: int, nslices: int):
+        """Walk only slice `slice_` of `nslices` key-ordered target slices; other targets' outputs
+        are zero (the slices of G ranks sum to the full result)."""
+        self._check(self.lib.gpugrav_set_target_slice(self._ctx, slice_, nslices))
+
     def set_stream(self, stream_handle: int | None):
         self._check(self.lib.gpugrav_set_stream(self._ctx, C.c_void_p(stream_handle) if stream_handle else None))
 

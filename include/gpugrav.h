@@ -175,6 +175,13 @@ int32_t gpugrav_build(gpugrav_ctx *ctx, const gpugrav_topnode *top, int32_t ntop
  * oldacc: n floats in caller order or NULL (zeros); acc: n*3 doubles; pot, ninter: n each or NULL.
  * All arrays in caller order, in memory of kind `mem`. */
 int32_t gpugrav_walk(gpugrav_ctx *ctx, const float *oldacc, double *acc, double *pot, int32_t *ninter, int32_t mem);
+/* Restrict the following walks (gpugrav_walk, gpugrav_compute) to slice `slice` of `nslices`
+ * contiguous slices of the targets in Peano-Hilbert order -- the reference's domain
+ * decomposition into key segments (src/domain/domain_toplevel.c), applied to targets only: the
+ * tree still holds every particle. FP32: slices are whole walk groups; FP64: target ranges.
+ * Outputs of targets outside the slice are written as zero, so the slices' outputs of G callers
+ * sum exactly to the unsliced result. Default 0 of 1 (all targets). */
+int32_t gpugrav_set_target_slice(gpugrav_ctx *ctx, int32_t slice, int32_t nslices);
 
 /* ---- one call: load + build + walk (the drop-in for construct_forcetree + gravity_tree) ---- */
 int32_t gpugrav_compute(gpugrav_ctx *ctx, int64_t n, const double *pos, const double *mass, const uint8_t *softtype,
