@@ -17,9 +17,12 @@ the same metric through the C ABI with host buffers (uploads and downloads insid
 the timed region).  Inputs (positions, tree, walk layout: > 2 GB) exceed the 126 MB
 L2, so no flush is needed between steps.
 
-With --gpus N (torchrun, one process per GPU) every rank runs its own
-independent zoom box (seed + rank): replicas, weak scaling, no collective on
-the data path; the step time is the maximum over ranks.
+With --gpus N (torchrun, one process per GPU) the same zoom box (N = 2^24 in
+total) is sharded: every rank owns 1/N of the particles, a step all-gathers the
+particles over NCCL, builds the same tree on every GPU, walks the rank's own
+key-ordered slice of the targets and reduce-scatters the forces to their owners
+(arepo_b200/sharded.py).  Total work is fixed: strong scaling; the step time is
+the maximum over ranks.
 
 Serving leg (rank 0 at N=1; --no-serving skips it): a seeded stream of isolated
 systems (Plummer spheres and Hernquist haloes, 50/50, N log-uniform in
@@ -65,7 +68,7 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-def workload_config(log2_half, precision, alpha):
+def workload_config(log2_half, precision, alpha, world=1):
     return {
         "workload": f"zoom box N=2^{log2_half + 1}: 2^{log2_half} uniform (mass 8m) + 2^{log2_half} Plummer b=0.02 r<0.1 "
                     f"(mass m), periodic L=1, PMGRID=512, RCUT=4.5, ASMTH=1.25, 2 softening types, relative criterion "
@@ -76,7 +79,9 @@ def workload_config(log2_half, precision, alpha):
         "walk_precision": precision,
         "l2": "inputs larger than L2 (no flush)",
         "global_batch": 1 << (log2_half + 1),
-        "parallelism": "replicas",
+        "parallelism": "one GPU" if world == 1 else
+                       f"one system sharded over {world} GPUs: all-gather of particles (NCCL), identical trees, "
+                       f"one key-ordered target slice per GPU, reduce-scatter of forces",
     }
 
 
@@ -212,7 +217,7 @@ def reference_arm(args):
     value = float(np.mean(vals))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * detail["n"] / value, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": 1e3 * detail["n"] / value, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": dict(workload_config(23, "fp64", args.err_tol_force_acc), cpu_sample=f"N=2^{CPU_SAMPLE_LOG2_HALF + 1} of the same zoom "
                        f"distribution, 1/{CPU_SAMPLE_STRIDE} of targets walked and extrapolated"),
@@ -392,6 +397,125 @@ def serving_leg(args, device):
 # --------------------------------------------------------------------------------------
 # our arm
 # --------------------------------------------------------------------------------------
+def sharded_arm(args):
+    """N > 1: one zoom box sharded over the ranks (see the module docstring)."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from arepo_b200 import _lib as L
+    from arepo_b200 import ics
+    from arepo_b200.sharded import ShardedGravity
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    os.environ.setdefault("MASTER_PORT", "29541")
+    os.environ.setdefault("RANK", str(rank))
+    os.environ.setdefault("WORLD_SIZE", str(world))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    prec = L.PREC_FP32 if args.precision == "fp32" else L.PREC_FP64
+    lh = args.log2_half
+    ic = ics.zoom_box(log2_half=lh, seed=1004, pmgrid=512)
+    n = len(ic["mass"])
+    lo, hi = n * rank // world, n * (rank + 1) // world
+    pos_h = torch.from_numpy(ic["pos"][lo:hi].copy()).pin_memory()
+    mass_h = torch.from_numpy(ic["mass"][lo:hi].copy()).pin_memory()
+    st_h = torch.from_numpy(ic["softtype"][lo:hi].copy()).pin_memory()
+    pos_d, mass_d, st_d = pos_h.to(dev), mass_h.to(dev), st_h.to(dev)
+    prm = ics.params_for(ic, precision=prec)
+    sg = ShardedGravity(prm, device=local)
+    tree = sg._tree
+    stream = torch.cuda.current_stream()
+
+    acc_d, _ = sg.compute(pos_d, mass_d, st_d, None)  # Barnes-Hut pass -> OldAcc
+    oldacc_d = torch.linalg.norm(acc_d, dim=1).to(torch.float32)
+    prm.err_tol_theta = 0.0
+    prm.err_tol_force_acc = args.err_tol_force_acc
+    tree.set_params(prm)
+    for _ in range(args.warmup):
+        acc_d, _ = sg.compute(pos_d, mass_d, st_d, oldacc_d)
+    torch.cuda.synchronize()
+
+    def timed(fn):
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        dist.barrier()
+        torch.cuda.synchronize()
+        start.record(stream)
+        for _ in range(args.steps):
+            fn()
+        end.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        t = torch.tensor([start.elapsed_time(end) / args.steps], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    walk_ms, inter = [], []
+
+    def step():
+        sg.compute(pos_d, mass_d, st_d, oldacc_d)
+        tm = tree.timings()
+        walk_ms.append(tm.walk_ms)
+        inter.append(tm.interactions)
+
+    with ClockSampler(local) as clk:
+        ms = timed(step)
+    old_h = oldacc_d.cpu().pin_memory()
+    acc_h = torch.empty((hi - lo, 3), dtype=torch.float64).pin_memory()
+
+    def step_e2e():
+        a, _ = sg.compute(pos_h.to(dev, non_blocking=True), mass_h.to(dev, non_blocking=True),
+                          st_h.to(dev, non_blocking=True), old_h.to(dev, non_blocking=True))
+        acc_h.copy_(a, non_blocking=True)
+
+    ms_e2e = timed(step_e2e)
+
+    line = None
+    if rank == 0:
+        rng = np.random.default_rng(2004)
+        tg = np.sort(rng.choice(hi - lo, min(8192, hi - lo), replace=False))
+        acc_tree = acc_h.numpy()[tg]
+        d_cut, _ = tree.direct(tg, cut=True)  # the tree context holds all particles, rank order = input order
+        dn = np.linalg.norm(d_cut, axis=1)
+        rel = np.linalg.norm(acc_tree - d_cut, axis=1) / np.maximum(dn, 1e-300)
+        pk = L.C.c_double(0.0)
+        tree.lib.gpugrav_measure_fma_peak(local, prec, L.C.byref(pk))
+        peak = float(pk.value)
+        walk_s = float(np.mean(walk_ms)) * 1e-3
+        ia = float(np.mean(inter))
+        achieved = FLOPS_PER_INTERACTION * ia / walk_s / 1e12
+        line = {
+            "metric": METRIC, "value": n / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32" if prec == L.PREC_FP32 else "f64", "data": "synthetic (seeded zoom box, arepo_b200/ics.py)",
+            "config": workload_config(lh, args.precision, args.err_tol_force_acc, world),
+            "roofline": {"bound": "fp32" if prec == L.PREC_FP32 else "fp64", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak if peak > 0 else None,
+                         "traffic": WALK32_DRAM_BYTES_PER_PARTICLE * n / world if prec == L.PREC_FP32 else None,
+                         "kernel": "k_walk32" if prec == L.PREC_FP32 else "k_walk64",
+                         "scope": "rank 0's walk of its target slice",
+                         "walk_ms": float(np.mean(walk_ms)), "interactions_per_step": ia},
+            "e2e": {"value": n / (ms_e2e * 1e-3), "unit": UNIT, "ms_per_step": ms_e2e,
+                    "h2d_bytes_per_step": world * (hi - lo) * (24 + 8 + 1 + 4),
+                    "d2h_bytes_per_step": world * (hi - lo) * 24},
+            "gpu_launches": int((5 + tree.timings().build_kernel_launches + 4) * args.steps),
+            "clocks": clk.report(),
+            "accuracy": {"rms_rel": float(np.sqrt(np.mean(rel * rel))), "p99_rel": float(np.percentile(rel, 99)),
+                         "targets": int(len(tg)), "reference": "FP64 direct sum over pairs closer than Rcut, rank 0's particles"},
+        }
+    sg.close()
+    dist.barrier()
+    dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def our_arm(args):
     import torch
 
@@ -549,7 +673,7 @@ def our_arm(args):
     e2e_value = world * n / (ms_e2e * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32" if prec == L.PREC_FP32 else "f64", "data": "synthetic (seeded zoom box, arepo_b200/ics.py)",
         "config": workload_config(lh, args.precision, args.err_tol_force_acc),
         "roofline": roofline,
@@ -599,6 +723,8 @@ def main():
     ap.add_argument("--log2-half", type=int, default=23, help="log2 of each species' count (23 -> N=2^24)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--sharded", action="store_true",
+                    help="use the sharded multi-GPU form also with one rank (it is the default for N > 1)")
     ap.add_argument("--serve-requests", type=int, default=160, help="requests in the Poisson serving stream")
     ap.add_argument("--serve-compare", type=int, default=48,
                     help="first requests of the stream timed batched and one at a time")
@@ -609,6 +735,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return reference_arm(args)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1 or args.sharded:
+        return sharded_arm(args)
     return our_arm(args)
 
 
