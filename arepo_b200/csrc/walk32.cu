@@ -193,6 +193,15 @@ __device__ __forceinline__ int wscan_incl(int v, int lane)
   return v;
 }
 
+// Reciprocal square root of a normal (never subnormal) argument: the hardware approximation
+// without the subnormal handling that a general rsqrtf needs (the walk clamps r^2 >= 1e-30).
+__device__ __forceinline__ float rsqrt_normal(float x)
+{
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // Table index without conversion instructions: adding 1.5 * 2^23 leaves round(te - 0.5)
 // (= floor(te) up to ties, where both neighbours give the same interpolated value) in the
 // low mantissa bits.
@@ -223,7 +232,7 @@ __device__ __forceinline__ void interact(const float4 e, const float hj, Tgt &T,
   const float hmax = fmaxf(T.h, hj);
   // a zero separation (the target itself) gives a huge rinv but r = 0: the spline branch,
   // whose periodic term is skipped at r = 0, handles it
-  const float rinv = rsqrtf(fmaxf(r2, 1.0e-30f));
+  const float rinv = rsqrt_normal(fmaxf(r2, 1.0e-30f));
   const float r    = r2 * rinv;
   bool in          = true;
   float ff = 0.0f, fpt = 0.0f;
