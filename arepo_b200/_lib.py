@@ -145,6 +145,7 @@ class Timings(C.Structure):
         ("interactions", C.c_int64),
         ("walk_kernel_launches", C.c_int32),
         ("build_kernel_launches", C.c_int32),
+        ("pm_ms", C.c_double),
     ]
 
 
@@ -162,6 +163,7 @@ _SIGS = {
     "gpugrav_build": (C.c_int32, [_P, _P, C.c_int32]),
     "gpugrav_walk": (C.c_int32, [_P, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_set_target_slice": (C.c_int32, [_P, C.c_int32, C.c_int32]),
+    "gpugrav_pm_periodic": (C.c_int32, [_P, C.c_int32, C.c_int64, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_compute": (C.c_int32, [_P, C.c_int64, _P, _P, _P, _P, C.POINTER(Domain), _P, C.c_int32, _P, _P, _P, C.c_int32]),
     "gpugrav_get_domain": (C.c_int32, [_P, C.POINTER(Domain)]),
     "gpugrav_get_order": (C.c_int32, [_P, _P]),

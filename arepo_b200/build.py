@@ -17,6 +17,7 @@ LIB = os.path.join(HERE, "libarepo_gpugrav.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+CUDA_LIB = os.path.join(os.path.dirname(os.path.dirname(NVCC)), "lib64")  # cuFFT (PM long-range force)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-I", INCLUDE, "-I", CSRC]
 
@@ -30,6 +31,7 @@ SOURCES = [
     ("walk32.cu", False),
     ("peak.cu", False),
     ("serve.cu", False),
+    ("pm.cu", False),
     ("gpugrav.cu", True),
 ]
 
@@ -56,7 +58,8 @@ def build(verbose: bool = False, force: bool = False, extra: list[str] | None = 
                 print(" ".join(cmd), file=sys.stderr)
             subprocess.check_call(cmd)
     if force or _needs(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-L" + CUDA_LIB, "-lcufft",
+                                                              "-Xlinker", "-rpath," + CUDA_LIB]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.check_call(cmd)

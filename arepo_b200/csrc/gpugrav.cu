@@ -337,7 +337,9 @@ int32_t gpugrav_destroy(gpugrav_ctx *c)
                         &c->n_next, &c->n_dfs, &c->n_first, &c->p_next, &c->p_father, &c->p_dfs, &c->depth_hist,
                         &c->depth_order, &c->w_sm, &c->w_cl, &c->w_link, &c->g_key, &c->g_key_alt, &c->g_val, &c->g_val_alt, &c->g_bfs, &c->g_np, &c->g_poff, &c->g_sm, &c->g_rel, &c->g_kids, &c->g_pm, &c->g_pst, &c->g_stack, &c->acc_s, &c->pot_s,
                         &c->nint_s, &c->oldacc_s, &c->oldacc_in, &c->out_acc, &c->out_pot, &c->out_nint, &c->scratch,
-                        &c->g_groups, &c->g_ngroups, &c->g_gpd, &c->g_gseg, &c->g_gflag, &c->g_gid, &c->m_sys, &c->m_doms};
+                        &c->g_groups, &c->g_ngroups, &c->g_gpd, &c->g_gseg, &c->g_gflag, &c->g_gid, &c->m_sys, &c->m_doms,
+                        &c->pm_pos, &c->pm_mass, &c->pm_acc, &c->pm_pot};
+  gg::pm_release(c);
   for(auto *b : bufs)
     b->release();
   c->pinned.release();
@@ -501,6 +503,56 @@ int32_t gpugrav_build(gpugrav_ctx *c, const gpugrav_topnode *top, int32_t ntop)
   c->timings.toptree_ms = elapsed(c->ev[4], c->ev[5]);
   c->timings.build_ms   = elapsed(c->ev[5], c->ev[6]);
   c->built              = true;
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_pm_periodic(gpugrav_ctx *c, int32_t pmgrid, int64_t n, const double *pos, const double *mass, double *acc,
+                            double *pot, int32_t mem)
+{
+  if(!c)
+    return GPUGRAV_ERR_INVALID;
+  if(pmgrid < 8 || pmgrid > 2048 || n < 0 || (n > 0 && (!pos || !mass || !acc)) ||
+     (mem != GPUGRAV_MEM_HOST && mem != GPUGRAV_MEM_DEVICE))
+    return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_pm_periodic: need 8 <= pmgrid <= 2048 and pos, mass, acc");
+  if(!c->prm.periodic || !(c->prm.box_size > 0) || !(c->prm.asmth > 0))
+    return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_pm_periodic: needs a periodic context with box_size > 0 and asmth > 0");
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->stream;
+  const double *d_pos = pos, *d_mass = mass;
+  double *d_acc = acc, *d_pot = pot;
+  if(mem == GPUGRAV_MEM_HOST)
+    {
+      if(c->pm_pos.ensure(n * 24 + 16) != cudaSuccess || c->pm_mass.ensure(n * 8 + 16) != cudaSuccess ||
+         c->pm_acc.ensure(n * 24 + 16) != cudaSuccess || (pot && c->pm_pot.ensure(n * 8 + 16) != cudaSuccess))
+        return fail(c, GPUGRAV_ERR_OOM, "gpugrav_pm_periodic: device allocation");
+      CK(cudaMemcpyAsync(c->pm_pos.p, pos, n * 24, cudaMemcpyHostToDevice, st), "upload positions");
+      CK(cudaMemcpyAsync(c->pm_mass.p, mass, n * 8, cudaMemcpyHostToDevice, st), "upload masses");
+      d_pos  = c->pm_pos.as<double>();
+      d_mass = c->pm_mass.as<double>();
+      d_acc  = c->pm_acc.as<double>();
+      d_pot  = pot ? c->pm_pot.as<double>() : nullptr;
+    }
+  cudaEventRecord(c->ev[18], st);
+  int fft_status = 0;
+  CK(gg::pm_stage(c, pmgrid, n, d_pos, d_mass, d_acc, d_pot, &fft_status), "pm");
+  cudaEventRecord(c->ev[19], st);
+  if(fft_status != 0)
+    {
+      const std::string m = "gpugrav_pm_periodic: cuFFT error " + std::to_string(fft_status);
+      return fail(c, GPUGRAV_ERR_CUDA, m.c_str());
+    }
+  if(mem == GPUGRAV_MEM_HOST)
+    {
+      CK(cudaMemcpyAsync(acc, d_acc, n * 24, cudaMemcpyDeviceToHost, st), "download acc");
+      if(pot)
+        CK(cudaMemcpyAsync(pot, d_pot, n * 8, cudaMemcpyDeviceToHost, st), "download pot");
+    }
+  int bad = 0;
+  CK(cudaMemcpyAsync(&bad, c->counters.as<int>() + 15, 4, cudaMemcpyDeviceToHost, st), "pm flags");
+  CK(cudaStreamSynchronize(st), "pm");
+  c->timings.pm_ms = elapsed(c->ev[18], c->ev[19]);
+  if(bad)
+    return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_pm_periodic: non-finite position or position far outside the box");
   return GPUGRAV_OK;
 }
 

@@ -136,6 +136,9 @@ struct gpugrav_ctx
   gg::DevBuf g_groups, g_ngroups;             // walk groups (first, count, root, criterion), their count
   gg::DevBuf g_gpd, g_gseg, g_gflag, g_gid;   // group construction scratch
   int32_t slice = 0, nslices = 1;             // target slice of the walks (gpugrav_set_target_slice)
+  // periodic PM long-range force (pm.cu): mesh size of the cuFFT plans, plans, meshes, particles
+  int32_t pm_grid = 0, pm_plan_f = 0, pm_plan_b = 0;
+  gg::DevBuf pm_rho, pm_rhok, pm_pos, pm_mass, pm_acc, pm_pot;
   int group_slack = 99;                       // group cuts between cells (< 64) or key order only (GPUGRAV_GROUP_SLACK)
   bool layout32_valid = false;
   // several independent systems in one build (serving): system of each sorted particle, domain of
@@ -171,6 +174,9 @@ cudaError_t walk32_prepare(gpugrav_ctx *c, const WalkConst &wc);
 cudaError_t walk32_launch(gpugrav_ctx *c);
 cudaError_t groups_stage(gpugrav_ctx *c);
 cudaError_t slice_mask_stage(gpugrav_ctx *c, bool fp32);
+cudaError_t pm_stage(gpugrav_ctx *c, int pmgrid, int64_t np, const double *pos, const double *mass, double *acc, double *pot,
+                     int *cufft_status);
+void pm_release(gpugrav_ctx *c);
 cudaError_t layout32_buffers(gpugrav_ctx *c, int64_t n, int64_t nn);
 cudaError_t layout32_reserve(gpugrav_ctx *c, int64_t n, int64_t nn);
 cudaError_t build_reserve(gpugrav_ctx *c, int64_t n, int64_t nn, int32_t ntop);

@@ -59,6 +59,23 @@ class GravityTree:
         self._check(self.lib.gpugrav_set_params(self._ctx, C.byref(params)))
         self.params = params
 
+    def pm_periodic(self, pmgrid: int, pos, mass, want_pot: bool = True, mem: int = L.MEM_HOST):
+        """Long-range periodic PM accelerations (without G) and potentials, as pmforce_periodic
+        (src/gravity/pm/pm_periodic.c:1572-1936); uses this context's box_size and asmth."""
+        if mem == L.MEM_HOST:
+            pos = np.ascontiguousarray(pos, np.float64)
+            mass = np.ascontiguousarray(mass, np.float64)
+            acc = np.empty((len(mass), 3), np.float64)
+            pot = np.empty(len(mass), np.float64) if want_pot else None
+        else:
+            import torch
+
+            acc = torch.empty((mass.shape[0], 3), dtype=torch.float64, device=pos.device)
+            pot = torch.empty(mass.shape[0], dtype=torch.float64, device=pos.device) if want_pot else None
+        self._check(self.lib.gpugrav_pm_periodic(self._ctx, pmgrid, len(mass) if mem == L.MEM_HOST else mass.shape[0],
+                                                 L.ptr(pos), L.ptr(mass), L.ptr(acc), L.ptr(pot), mem))
+        return acc, pot
+
     def set_target_slice(self, slice_: int, nslices: int):
         """Walk only slice `slice_` of `nslices` key-ordered target slices; other targets' outputs
         are zero (the slices of G ranks sum to the full result)."""

@@ -129,6 +129,7 @@ typedef struct gpugrav_timings
   int64_t interactions; /* sum of per-target interaction counts of the last walk */
   int32_t walk_kernel_launches;
   int32_t build_kernel_launches;
+  double pm_ms; /* last gpugrav_pm_periodic: deposit, FFTs, Green's function, readout */
 } gpugrav_timings;
 
 typedef struct gpugrav_ctx gpugrav_ctx;
@@ -182,6 +183,16 @@ int32_t gpugrav_walk(gpugrav_ctx *ctx, const float *oldacc, double *acc, double 
  * Outputs of targets outside the slice are written as zero, so the slices' outputs of G callers
  * sum exactly to the unsliced result. Default 0 of 1 (all targets). */
 int32_t gpugrav_set_target_slice(gpugrav_ctx *ctx, int32_t slice, int32_t nslices);
+
+/* Long-range periodic PM accelerations (without G) and potentials of n particles; replaces
+ * pmforce_periodic(0, NULL) (src/gravity/pm/pm_periodic.c:1572-1936): CIC assignment on a
+ * pmgrid^3 mesh, FFT, Green's function -exp(-k^2 Asmth^2)/k^2 with the CIC deconvolution, inverse
+ * FFT, 4-point finite differences, CIC readout (FP64 mesh). Uses the context's box_size and asmth
+ * (Asmth = ASMTH * BoxSize / PMGRID); positions in [0, box_size); independent of the tree state.
+ * pos n*3, mass n, acc n*3 (required), pot n (may be NULL); host or device arrays per `mem`.
+ * 8 <= pmgrid <= 2048. */
+int32_t gpugrav_pm_periodic(gpugrav_ctx *ctx, int32_t pmgrid, int64_t n, const double *pos, const double *mass, double *acc,
+                            double *pot, int32_t mem);
 
 /* ---- one call: load + build + walk (the drop-in for construct_forcetree + gravity_tree) ---- */
 int32_t gpugrav_compute(gpugrav_ctx *ctx, int64_t n, const double *pos, const double *mass, const uint8_t *softtype,
