@@ -60,7 +60,8 @@ typedef unsigned __int128 u128;
 /* ------------------------------------------------------------------------ */
 typedef struct
 {
-  int periodic;      /* 1: periodic TreePM (PMGRID build); 0: isolated (GRAVITY_NOT_PERIODIC) */
+  int periodic;      /* 1: periodic: TreePM (PMGRID build) if asmth > 0, else pure tree with Ewald
+                        correction (periodic build without PMGRID); 0: isolated (GRAVITY_NOT_PERIODIC) */
   int nsoft;         /* NSOFTTYPES; ForceSoftening has nsoft+1 entries, the last one 0 */
   double box;        /* All.BoxSize */
   double asmth;      /* All.Asmth[0] */
@@ -816,6 +817,178 @@ static inline double nearest(double x, const or_params *p)
   return (x > half) ? (x - p->box) : ((x < -half) ? (x + p->box) : x);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Ewald correction of the periodic pure-tree walk (no PMGRID):             */
+/* src/gravity/forcetree_ewald.c                                            */
+/* ------------------------------------------------------------------------ */
+#define OR_EN 64
+
+/* ewald_psi, forcetree_ewald.c:393-461 (cubic box, STRETCH = 1) */
+static double or_ewald_psi(double x, double y, double z)
+{
+  double r = sqrt(x * x + y * y + z * z);
+  if(r == 0)
+    return 0;
+  double alpha   = 3.0;
+  const int nmax = 4;
+  double sum1    = 0;
+  for(int nx = -nmax; nx <= nmax; nx++)
+    for(int ny = -nmax; ny <= nmax; ny++)
+      for(int nz = -nmax; nz <= nmax; nz++)
+        {
+          double dx = x - nx, dy = y - ny, dz = z - nz;
+          double rr = sqrt(dx * dx + dy * dy + dz * dz);
+          sum1 += erfc(alpha * rr) / rr;
+        }
+  double alpha2 = alpha * alpha;
+  int kmax      = (int)(2 * alpha + 0.5);
+  double sum2   = 0.0;
+  for(int nx = -kmax; nx <= kmax; nx++)
+    for(int ny = -kmax; ny <= kmax; ny++)
+      for(int nz = -kmax; nz <= kmax; nz++)
+        {
+          double kx = (2.0 * M_PI) * nx, ky = (2.0 * M_PI) * ny, kz = (2.0 * M_PI) * nz;
+          double k2 = kx * kx + ky * ky + kz * kz;
+          if(k2 > 0)
+            {
+              double kdotx = (x * kx + y * ky + z * kz);
+              sum2 += 4.0 * M_PI / k2 * exp(-k2 / (4.0 * alpha2)) * cos(kdotx);
+            }
+        }
+  return M_PI / (alpha * alpha) - sum1 - sum2 + 1.0 / r;
+}
+
+/* ewald_force, forcetree_ewald.c:463-527 */
+static void or_ewald_force(double x, double y, double z, double force[3])
+{
+  for(int i = 0; i < 3; i++)
+    force[i] = 0;
+  double r2 = x * x + y * y + z * z;
+  if(r2 == 0)
+    return;
+  double alpha  = 2.0;
+  double alpha2 = alpha * alpha;
+  double r3inv  = 1.0 / (r2 * sqrt(r2));
+  force[0] += r3inv * x;
+  force[1] += r3inv * y;
+  force[2] += r3inv * z;
+  const int nmax = 4;
+  for(int nx = -nmax; nx <= nmax; nx++)
+    for(int ny = -nmax; ny <= nmax; ny++)
+      for(int nz = -nmax; nz <= nmax; nz++)
+        {
+          double dx   = x - nx, dy = y - ny, dz = z - nz;
+          double rr2  = dx * dx + dy * dy + dz * dz;
+          double r    = sqrt(rr2);
+          double val  = erfc(alpha * r) + 2.0 * alpha * r / sqrt(M_PI) * exp(-alpha2 * rr2);
+          double val2 = val / (rr2 * r);
+          force[0] -= dx * val2;
+          force[1] -= dy * val2;
+          force[2] -= dz * val2;
+        }
+  int hmax = (int)(2 * alpha + 0.5);
+  for(int hx = -hmax; hx <= hmax; hx++)
+    for(int hy = -hmax; hy <= hmax; hy++)
+      for(int hz = -hmax; hz <= hmax; hz++)
+        {
+          double h2 = hx * hx + hy * hy + hz * hz;
+          if(h2 > 0)
+            {
+              double hdotx = x * hx + y * hy + z * hz;
+              double val   = 2.0 / h2 * exp(-M_PI * M_PI * h2 / alpha2) * sin(2.0 * M_PI * hdotx);
+              force[0] -= hx * val;
+              force[1] -= hy * val;
+              force[2] -= hz * val;
+            }
+        }
+}
+
+/* The unscaled tables of ewald_init (forcetree_ewald.c:154-185): one octant of the unit box, entry
+ * (i, j, k) at (i, j, k) / (2 EN); (EN + 1)^3 values each, k fastest. */
+void or_ewald_table(double *fx, double *fy, double *fz, double *pot)
+{
+  const int m = OR_EN + 1;
+#pragma omp parallel for schedule(dynamic, 64)
+  for(int n = 0; n < m * m * m; n++)
+    {
+      int i = n / (m * m), j = (n - i * m * m) / m, k = n - i * m * m - j * m;
+      double xx = 0.5 * ((double)i) / OR_EN, yy = 0.5 * ((double)j) / OR_EN, zz = 0.5 * ((double)k) / OR_EN;
+      double f[3];
+      pot[n] = or_ewald_psi(xx, yy, zz);
+      or_ewald_force(xx, yy, zz, f);
+      fx[n] = f[0];
+      fy[n] = f[1];
+      fz[n] = f[2];
+    }
+}
+
+static const double *or_ewd_fx, *or_ewd_fy, *or_ewd_fz, *or_ewd_pot; /* scaled to the box */
+static double or_ewd_fac_intp;
+
+/* the tables scaled to the box as at the end of ewald_init (forcetree_ewald.c:239-251); the caller
+ * keeps the arrays alive */
+void or_set_ewald_table(double box, const double *fx, const double *fy, const double *fz, const double *pot)
+{
+  or_ewd_fx = fx, or_ewd_fy = fy, or_ewd_fz = fz, or_ewd_pot = pot;
+  or_ewd_fac_intp = 2 * OR_EN / box;
+}
+
+#define OR_EI(i, j, k) (((i) * (OR_EN + 1) + (j)) * (OR_EN + 1) + (k))
+
+/* ewald_corr and ewald_pot_corr, forcetree_ewald.c:268-391 */
+static void or_ewald_corr(double dx, double dy, double dz, double *fper, double *pcorr)
+{
+  int signx, signy, signz;
+  if(dx < 0)
+    {
+      dx    = -dx;
+      signx = +1;
+    }
+  else
+    signx = -1;
+  if(dy < 0)
+    {
+      dy    = -dy;
+      signy = +1;
+    }
+  else
+    signy = -1;
+  if(dz < 0)
+    {
+      dz    = -dz;
+      signz = +1;
+    }
+  else
+    signz = -1;
+  double u = dx * or_ewd_fac_intp;
+  int i    = (int)u;
+  if(i >= OR_EN)
+    i = OR_EN - 1;
+  u -= i;
+  double v = dy * or_ewd_fac_intp;
+  int j    = (int)v;
+  if(j >= OR_EN)
+    j = OR_EN - 1;
+  v -= j;
+  double w = dz * or_ewd_fac_intp;
+  int k    = (int)w;
+  if(k >= OR_EN)
+    k = OR_EN - 1;
+  w -= k;
+  double f1 = (1 - u) * (1 - v) * (1 - w), f2 = (1 - u) * (1 - v) * (w), f3 = (1 - u) * (v) * (1 - w), f4 = (1 - u) * (v) * (w);
+  double f5 = (u) * (1 - v) * (1 - w), f6 = (u) * (1 - v) * (w), f7 = (u) * (v) * (1 - w), f8 = (u) * (v) * (w);
+  const double *t[4] = {or_ewd_fx, or_ewd_fy, or_ewd_fz, or_ewd_pot};
+  double r[4];
+  for(int c = 0; c < 4; c++)
+    r[c] = t[c][OR_EI(i, j, k)] * f1 + t[c][OR_EI(i, j, k + 1)] * f2 + t[c][OR_EI(i, j + 1, k)] * f3 +
+           t[c][OR_EI(i, j + 1, k + 1)] * f4 + t[c][OR_EI(i + 1, j, k)] * f5 + t[c][OR_EI(i + 1, j, k + 1)] * f6 +
+           t[c][OR_EI(i + 1, j + 1, k)] * f7 + t[c][OR_EI(i + 1, j + 1, k + 1)] * f8;
+  fper[0] = signx * r[0];
+  fper[1] = signy * r[1];
+  fper[2] = signz * r[2];
+  *pcorr  = r[3];
+}
+
 void or_walk(int64_t ntargets, const int64_t *targets, const double *tpos, const float *oldacc, const uint8_t *tstype,
              const double *pos, const double *mass, const uint8_t *stype, const int32_t *p_next, int64_t max_part,
              int64_t num_nodes, const double *center, const double *len, const double *s, const double *nmass,
@@ -823,10 +996,13 @@ void or_walk(int64_t ntargets, const int64_t *targets, const double *tpos, const
              double *pot_out, int32_t *ninter_out)
 {
   float tab_f[OR_NTAB + 1], tab_p[OR_NTAB + 1];
-  or_shortrange_table(p->rcut_cells, tab_f, tab_p);
+  const int pm    = p->periodic && p->asmth > 0;  /* TreePM split */
+  const int ewald = p->periodic && !pm;           /* pure tree, Ewald-corrected */
+  if(pm)
+    or_shortrange_table(p->rcut_cells, tab_f, tab_p);
   const double rcut      = p->rcut;
   const double rcut2     = rcut * rcut;
-  const double asmthinv  = 0.5 / p->asmth;
+  const double asmthinv  = pm ? 0.5 / p->asmth : 0.0;
   const double asmthinv2 = asmthinv * asmthinv;
   const double asmthfac  = asmthinv * (OR_NTAB / (p->rcut_cells / 2.0));
 
@@ -862,7 +1038,7 @@ void or_walk(int64_t ntargets, const int64_t *targets, const double *tpos, const
               dy        = nearest(s[3 * k + 1] - pos_y, p);
               dz        = nearest(s[3 * k + 2] - pos_z, p);
               r2        = dx * dx + dy * dy + dz * dz;
-              if(p->periodic && r2 > rcut2)
+              if(pm && r2 > rcut2)
                 {
                   double eff_dist = rcut + 0.5 * len[k];
                   double dist     = nearest(center[3 * k + 0] - pos_x, p);
@@ -932,7 +1108,7 @@ void or_walk(int64_t ntargets, const int64_t *targets, const double *tpos, const
             {
               double r = sqrt(r2);
               double factor_force = 0, factor_pot = 0;
-              if(p->periodic)
+              if(pm)
                 {
                   double tabentry = asmthfac * r;
                   int tabindex    = (int)tabentry;
@@ -947,7 +1123,7 @@ void or_walk(int64_t ntargets, const int64_t *targets, const double *tpos, const
                 {
                   double rinv  = 1.0 / r;
                   double rinv3 = rinv * rinv * rinv;
-                  if(p->periodic)
+                  if(pm)
                     {
                       fac = rinv3 + rinv * factor_force * asmthinv2;
                       wp  = rinv * factor_pot;
@@ -976,7 +1152,7 @@ void or_walk(int64_t ntargets, const int64_t *targets, const double *tpos, const
                       fac       = h3_inv * (SF8 + SF9 * u + SF10 * u2 + SF11 * u3 + SF12 / u3);
                       wp        = h_inv * (SF13 + SF14 / u + u2 * (SF1 + u * (SF15 + u * (SF16 + SF17 * u))));
                     }
-                  if(p->periodic && r > 0)
+                  if(pm && r > 0)
                     {
                       double rinv = 1.0 / r;
                       fac += rinv * factor_force * asmthinv2;
@@ -988,6 +1164,15 @@ void or_walk(int64_t ntargets, const int64_t *targets, const double *tpos, const
               acc_x += dx * fac;
               acc_y += dy * fac;
               acc_z += dz * fac;
+              if(ewald)
+                {
+                  double fcorr[3], pcorr;
+                  or_ewald_corr(dx, dy, dz, fcorr, &pcorr);
+                  acc_x += m * fcorr[0];
+                  acc_y += m * fcorr[1];
+                  acc_z += m * fcorr[2];
+                  pot += m * pcorr;
+                }
               ninteractions++;
             }
         }
@@ -1053,7 +1238,7 @@ void or_direct(int64_t ntargets, const int64_t *targets, int64_t n, const double
                   wp  = m * h_inv * (SF13 + SF14 / u + u2 * (SF1 + u * (SF15 + u * (SF16 + SF17 * u))));
                 }
             }
-          if(p->periodic)
+          if(p->periodic && p->asmth > 0)
             {
               double u            = 0.5 / p->asmth * r;
               double factor_force = (erfc(u) + 2.0 * u / sqrt(M_PI) * exp(-u * u) - 1.0);
@@ -1065,6 +1250,16 @@ void or_direct(int64_t ntargets, const int64_t *targets, int64_t n, const double
           ay += dy * fac;
           az += dz * fac;
           pt += wp;
+          if(p->periodic && !(p->asmth > 0))
+            {
+              /* pure periodic tree: all images through the Ewald correction (forcetest with Ewald) */
+              double fcorr[3], pcorr;
+              or_ewald_corr(dx, dy, dz, fcorr, &pcorr);
+              ax += m * fcorr[0];
+              ay += m * fcorr[1];
+              az += m * fcorr[2];
+              pt += m * pcorr;
+            }
         }
       acc_out[3 * q + 0] = ax;
       acc_out[3 * q + 1] = ay;

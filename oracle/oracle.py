@@ -75,7 +75,7 @@ def build_oracle(force: bool = False) -> str:
     os.makedirs(BUILD_DIR, exist_ok=True)
     if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(SRC_PATH):
         subprocess.check_call(
-            ["gcc", "-std=gnu11", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", LIB_PATH, SRC_PATH, "-lm"]
+            ["gcc", "-std=gnu11", "-O2", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", "-o", LIB_PATH, SRC_PATH, "-lm"]
         )
     return LIB_PATH
 
@@ -113,7 +113,46 @@ def lib():
         _lib.or_shortrange_table.argtypes = [C.c_double, p, p]
         _lib.or_walk.argtypes = [i64, p, p, p, p, p, p, p, p, i64, i64, p, p, p, p, p, p, p, p, p, p, p]
         _lib.or_direct.argtypes = [i64, p, i64, p, p, p, p, p, p]
+        _lib.or_ewald_table.argtypes = [p, p, p, p]
+        _lib.or_set_ewald_table.argtypes = [C.c_double, p, p, p, p]
     return _lib
+
+
+EWALD_EN = 64
+_ewald_unscaled = None
+_ewald_scaled = {}
+
+
+def ewald_table():
+    """The unscaled Ewald correction tables of ewald_init (forcetree_ewald.c:154-185), computed by
+    the C restatement (about 30 CPU-seconds, OpenMP) and cached in oracle/_build."""
+    global _ewald_unscaled
+    if _ewald_unscaled is None:
+        f = os.path.join(BUILD_DIR, f"ewald_table_{EWALD_EN}.npy")
+        if os.path.exists(f):
+            _ewald_unscaled = np.load(f)
+        else:
+            m = (EWALD_EN + 1) ** 3
+            t = np.zeros((4, m))
+            lib().or_ewald_table(_ptr(t[0]), _ptr(t[1]), _ptr(t[2]), _ptr(t[3]))
+            os.makedirs(BUILD_DIR, exist_ok=True)
+            np.save(f, t)
+            _ewald_unscaled = t
+    return _ewald_unscaled
+
+
+def use_ewald(prm):
+    """Install the tables scaled to prm.box (fcorr / L^2, potcorr / L, forcetree_ewald.c:239-251) for
+    the walk and direct sum of a periodic pure-tree parameter set (periodic, asmth == 0)."""
+    if not (prm.periodic and prm.asmth == 0):
+        return
+    box = float(prm.box)
+    if box not in _ewald_scaled:
+        t = ewald_table()
+        _ewald_scaled[box] = np.ascontiguousarray(np.stack([t[0] / (box * box), t[1] / (box * box), t[2] / (box * box),
+                                                            t[3] / box]))
+    s = _ewald_scaled[box]
+    lib().or_set_ewald_table(box, _ptr(s[0]), _ptr(s[1]), _ptr(s[2]), _ptr(s[3]))
 
 
 def _ptr(a):
@@ -230,6 +269,7 @@ def build(pos_sorted, mass_sorted, st_sorted, ip_sorted, prm, dom, top, max_part
 
 
 def walk(tree, pos_sorted, mass_sorted, st_sorted, oldacc_sorted, prm, targets=None):
+    use_ewald(prm)
     n = len(mass_sorted)
     tg = None if targets is None else np.ascontiguousarray(targets, np.int64)
     nt = n if targets is None else len(tg)
@@ -250,6 +290,7 @@ def walk(tree, pos_sorted, mass_sorted, st_sorted, oldacc_sorted, prm, targets=N
 
 
 def direct(pos, mass, st, prm, targets):
+    use_ewald(prm)
     pos = np.ascontiguousarray(pos, np.float64)
     mass = np.ascontiguousarray(mass, np.float64)
     st = np.ascontiguousarray(st, np.uint8)
@@ -363,11 +404,17 @@ def read_output(path):
 
 def run_ref(pos, mass, st, periodic, *, box=1.0, asmth=None, rcut=None, theta=0.7, erracc=0.0025,
             softening=(0.01, 0.01), mdom=8, tnf=2.5, passes=2, dump=1, gt=1, first=0, count=None, stride=1,
-            timeout=3600):
-    """Run the compiled reference harness; returns the parsed dump."""
-    exe = os.path.join(REF_DIR, "ref_harness_pm" if periodic else "ref_harness_iso")
+            timeout=3600, ewald=False, ewald_table_out=None):
+    """Run the compiled reference harness; returns the parsed dump.  ewald=True: the periodic
+    pure-tree build (no PM, Ewald correction); its table file is cached in oracle/_ref/ewald_cache
+    (the reference writes it to the working directory), ewald_table_out dumps the scaled table."""
+    exe = os.path.join(REF_DIR, "ref_harness_ewald" if ewald else ("ref_harness_pm" if periodic else "ref_harness_iso"))
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
+    cwd = None
+    if ewald:
+        cwd = os.path.join(REF_DIR, "ewald_cache")
+        os.makedirs(cwd, exist_ok=True)
     with tempfile.TemporaryDirectory() as td:
         fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
         write_input(fin, pos, mass, st)
@@ -377,9 +424,11 @@ def run_ref(pos, mass, st, periodic, *, box=1.0, asmth=None, rcut=None, theta=0.
                 f"first={first}", f"stride={stride}"]
         if count is not None:
             args.append(f"count={count}")
-        if periodic:
+        if periodic and not ewald:
             args += [f"asmth={asmth!r}", f"rcut={rcut!r}"]
-        res = subprocess.run(args, capture_output=True, text=True, timeout=timeout)
+        if ewald_table_out:
+            args.append(f"ewaldout={ewald_table_out}")
+        res = subprocess.run(args, capture_output=True, text=True, timeout=timeout, cwd=cwd)
         if res.returncode != 0:
             raise RuntimeError(f"reference harness failed ({res.returncode}): {res.stdout[-2000:]} {res.stderr[-2000:]}")
         out = read_output(fout)

@@ -53,6 +53,15 @@ static double arg_d(int argc, char **argv, const char *key, double def)
   return def;
 }
 
+static const char *arg_s(int argc, char **argv, const char *key, const char *def)
+{
+  size_t l = strlen(key);
+  for(int i = 3; i < argc; i++)
+    if(strncmp(argv[i], key, l) == 0 && argv[i][l] == '=')
+      return argv[i] + l + 1;
+  return def;
+}
+
 static void wr(FILE *f, const void *p, size_t sz, size_t n)
 {
   if(n && fwrite(p, sz, n, f) != n)
@@ -253,6 +262,28 @@ int main(int argc, char **argv)
 #ifdef PMGRID
   All.Asmth[0] = arg_d(argc, argv, "asmth", 1.25 / PMGRID);
   All.Rcut[0]  = arg_d(argc, argv, "rcut", RCUT * All.Asmth[0]);
+#endif
+#if !defined(PMGRID) && !defined(GRAVITY_NOT_PERIODIC)
+  /* periodic pure-tree build: the reference's Ewald correction tables (forcetree_ewald.c:89-254),
+   * read from / written to ewald_table_64_64_64.dat in the working directory */
+  ewald_init();
+  {
+    const char *tabout = arg_s(argc, argv, "ewaldout", NULL);
+    if(tabout)
+      {
+        FILE *ft = fopen(tabout, "wb");
+        if(!ft)
+          return 1;
+        int64_t sz = (int64_t)(ENX + 1) * (ENY + 1) * (ENZ + 1);
+        wr(ft, &sz, 8, 1);
+        wr(ft, &Ewd_fac_intp, 8, 1);
+        wr(ft, Ewd_fcorrx, sizeof(MyFloat), sz);
+        wr(ft, Ewd_fcorry, sizeof(MyFloat), sz);
+        wr(ft, Ewd_fcorrz, sizeof(MyFloat), sz);
+        wr(ft, Ewd_potcorr, sizeof(MyFloat), sz);
+        fclose(ft);
+      }
+  }
 #endif
 
   double t0 = wall();

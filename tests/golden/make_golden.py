@@ -1,8 +1,8 @@
 """Generates the golden fixtures in this directory by running the reference's own
-gravity code (oracle/_ref/ref_harness_{pm,iso}, compiled from the reference tree
+gravity code (oracle/_ref/ref_harness_{pm,iso,ewald}, compiled from the reference tree
 by oracle/ref/Makefile) on small seeded particle sets.
 
-    python tests/golden/make_golden.py            # needs the reference tree to build the harness
+    python tests/golden/make_golden.py [case ...]  # needs the reference tree to build the harness
 
 Each fixture (.npz) holds the inputs, the run parameters and the reference's
 outputs: domain geometry, sorted order, 126-bit keys, top-level nodes, the full
@@ -12,12 +12,18 @@ per-particle accelerations, potentials, interaction counts and OldAcc.
 
 Node indices are stored with the library's convention Tree_MaxPart = N (the
 reference run uses All.MaxPart, which domain_Decomposition enlarges).
+
+The periodic pure-tree case (no PMGRID, Ewald-corrected) also stores the SHA-256 of the
+reference's scaled Ewald correction tables (ewald_init, forcetree_ewald.c:89-254) and a sample of
+their entries, which pins the table restatement without shipping the 8.8 MB tables.
 """
 from __future__ import annotations
 
+import hashlib
 import json
 import os
 import sys
+import tempfile
 
 import numpy as np
 
@@ -50,6 +56,11 @@ def cases():
     a = 1.25 / 64
     c["mix1500_pm"] = dict(pos=pos, mass=mass, softtype=st, softening=(0.001, 0.0003), periodic=True, box=1.0, asmth=a,
                            rcut=4.5 * a)
+    # periodic pure tree with Ewald correction: 12^3 grid + displacements in a box of size 2
+    g = ics.grid_box(n1=12, seed=1006, pmgrid=32)
+    c["grid12_ewald"] = dict(pos=2.0 * g["pos"], mass=g["mass"], softtype=g["softtype"],
+                             softening=tuple(2.0 * e for e in g["softening"]), periodic=True, box=2.0, asmth=0.0,
+                             rcut=0.0, ewald=True)
     return c
 
 
@@ -63,15 +74,21 @@ def remap(a, mp_ref, n):
 def main():
     if not O.build_ref():
         raise SystemExit("reference harness unavailable: the reference tree is needed to regenerate fixtures")
+    want = set(sys.argv[1:])
     for name, ic in cases().items():
+        if want and name not in want:
+            continue
         soft = tuple(ic["softening"]) + (ic["softening"][-1],) * (2 - len(ic["softening"]))
+        ewald = bool(ic.get("ewald", False))
+        tabf = tempfile.mktemp(suffix=".bin") if ewald else None
         ref = O.run_ref(ic["pos"], ic["mass"], ic["softtype"], ic["periodic"], box=ic["box"], asmth=ic["asmth"],
-                        rcut=ic["rcut"], theta=0.7, erracc=0.0025, softening=soft, mdom=8, tnf=2.5)
+                        rcut=ic["rcut"], theta=0.7, erracc=0.0025, softening=soft, mdom=8, tnf=2.5, ewald=ewald,
+                        ewald_table_out=tabf)
         n = len(ic["mass"])
         m = ref["tree_meta"]
         mp = m["max_part"]
         prm = dict(periodic=bool(ic["periodic"]), box=ic["box"], asmth=ic["asmth"], rcut=ic["rcut"], rcut_cells=4.5,
-                   softening=list(soft), theta=0.7, erracc=0.0025, mdom=8, tnf=2.5)
+                   softening=list(soft), theta=0.7, erracc=0.0025, mdom=8, tnf=2.5, ewald=ewald)
         out = dict(
             params=np.array(json.dumps(prm)),
             pos=ic["pos"], mass=ic["mass"], softtype=ic["softtype"],
@@ -82,6 +99,16 @@ def main():
             node_nextnode=remap(ref["node_nextnode"], mp, n), node_father=remap(ref["node_father"], mp, n),
             p_next=remap(ref["p_next"], mp, n), p_father=remap(ref["p_father"], mp, n),
         )
+        if ewald:
+            raw = open(tabf, "rb").read()
+            os.remove(tabf)
+            sz = int(np.frombuffer(raw[:8], np.int64)[0])
+            tab = np.frombuffer(raw[16:], np.float64).reshape(4, sz)
+            out["ewald_fac_intp"] = np.frombuffer(raw[8:16], np.float64)[0]
+            out["ewald_sha256"] = np.array(hashlib.sha256(tab.tobytes()).hexdigest())
+            idx = np.random.default_rng(7).choice(sz, 64, replace=False)
+            out["ewald_sample_idx"] = idx
+            out["ewald_sample"] = tab[:, idx]
         for ps in range(2):
             for k in ("acc", "pot", "ninter", "oldacc"):
                 out[f"{k}{ps}"] = ref[f"{k}{ps}"]

@@ -65,6 +65,20 @@ def test_oracle_top_tree_matches_reference(name):
     assert np.array_equal(t2["morton_to_peano"], g["top"]["morton_to_peano"])
 
 
+def test_ewald_tables_match_reference():
+    """The restated Ewald correction tables (ewald_init, forcetree_ewald.c:154-251) scaled to the
+    fixture's box: the same bytes as the reference's (SHA-256 and sampled entries)."""
+    import hashlib
+
+    g = load_golden("grid12_ewald")
+    box = g["params"]["box"]
+    t = O.ewald_table()
+    scaled = np.stack([t[0] / (box * box), t[1] / (box * box), t[2] / (box * box), t[3] / box])
+    assert np.array_equal(scaled[:, g["ewald_sample_idx"]], g["ewald_sample"])
+    assert hashlib.sha256(np.ascontiguousarray(scaled).tobytes()).hexdigest() == str(g["ewald_sha256"])
+    assert float(g["ewald_fac_intp"]) == 2 * O.EWALD_EN / box
+
+
 def test_shortrange_table_matches_reference_formula():
     f, p = O.shortrange_table(4.5)
     assert f[0] == 0.0 and p[0] == np.float32(-1.0)
