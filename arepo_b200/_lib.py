@@ -164,6 +164,7 @@ _SIGS = {
     "gpugrav_walk": (C.c_int32, [_P, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_set_target_slice": (C.c_int32, [_P, C.c_int32, C.c_int32]),
     "gpugrav_pm_periodic": (C.c_int32, [_P, C.c_int32, C.c_int64, _P, _P, _P, _P, C.c_int32]),
+    "gpugrav_set_ewald_table": (C.c_int32, [_P, C.c_int32, _P, _P, _P, _P]),
     "gpugrav_compute": (C.c_int32, [_P, C.c_int64, _P, _P, _P, _P, C.POINTER(Domain), _P, C.c_int32, _P, _P, _P, C.c_int32]),
     "gpugrav_get_domain": (C.c_int32, [_P, C.POINTER(Domain)]),
     "gpugrav_get_order": (C.c_int32, [_P, _P]),

@@ -32,6 +32,7 @@ SOURCES = [
     ("peak.cu", False),
     ("serve.cu", False),
     ("pm.cu", False),
+    ("ewald.cu", True),
     ("gpugrav.cu", True),
 ]
 

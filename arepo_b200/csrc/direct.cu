@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(kTile) k_direct(const double4 *__restrict__ pm
       me        = pm[i];
       h_i       = w.soft[st[i]];
     }
-  const double asmth = (w.periodic) ? (0.5 / sqrt(w.asmthinv2)) : 0.0;
+  const double asmth = (w.pm) ? (0.5 / sqrt(w.asmthinv2)) : 0.0;
   double ax = 0, ay = 0, az = 0, pt = 0;
   for(int64_t jb = j0; jb < j1; jb += kTile)
     {
@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(kTile) k_direct(const double4 *__restrict__ pm
                 dz = (dz > w.half_box) ? dz - w.box : ((dz < -w.half_box) ? dz + w.box : dz);
               }
             double r2 = dx * dx + dy * dy + dz * dz;
-            if(cut && w.periodic && !(r2 < w.rcut2))
+            if(cut && w.pm && !(r2 < w.rcut2))
               continue;  // beyond Rcut: the part of the force left to the PM mesh
             double r  = sqrt(r2);
             double m  = s.w;
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(kTile) k_direct(const double4 *__restrict__ pm
                     wp  = m * h_inv * (SF13 + SF14 / u + u2 * (SF1 + u * (SF15 + u * (SF16 + SF17 * u))));
                   }
               }
-            if(w.periodic)
+            if(w.pm)
               {
                 double u            = 0.5 / asmth * r;
                 double factor_force = (erfc(u) + 2.0 * u / sqrt(M_PI) * exp(-u * u) - 1.0);
@@ -121,6 +121,16 @@ __global__ void __launch_bounds__(kTile) k_direct(const double4 *__restrict__ pm
             ay += dy * fac;
             az += dz * fac;
             pt += wp;
+            if(w.ewald)
+              {
+                // pure periodic tree: every image through the Ewald correction
+                double fcorr[3], pcorr;
+                ewald_corr(dx, dy, dz, w, fcorr, pcorr);
+                ax += m * fcorr[0];
+                ay += m * fcorr[1];
+                az += m * fcorr[2];
+                pt += m * pcorr;
+              }
           }
     }
   if(t < nt)

@@ -131,8 +131,9 @@ int validate_params(const gpugrav_params *p)
       return GPUGRAV_ERR_INVALID;
   if(!(p->box_size > 0) || !std::isfinite(p->box_size))
     return GPUGRAV_ERR_INVALID;
-  if(p->periodic)
+  if(p->periodic && p->asmth != 0.0)
     {
+      // TreePM split; asmth == 0 selects the pure periodic tree with Ewald correction
       if(!(p->asmth > 0) || !(p->rcut > 0) || !(p->rcut_cells > 0))
         return GPUGRAV_ERR_INVALID;
     }
@@ -206,6 +207,10 @@ void gg::make_walk_const(const gpugrav_params &p, WalkConst *w)
 {
   memset(w, 0, sizeof(*w));
   w->periodic = p.periodic;
+  w->pm       = p.periodic && p.asmth > 0;
+  w->ewald    = p.periodic && !(p.asmth > 0);
+  if(w->ewald)
+    w->ewd_fac_intp = 2.0 * gg::kEwaldN / p.box_size;
   w->bh       = p.err_tol_theta > 0 ? 1 : 0;
   w->box      = p.box_size;
   w->half_box = 0.5 * p.box_size;
@@ -213,7 +218,7 @@ void gg::make_walk_const(const gpugrav_params &p, WalkConst *w)
   w->erracc   = p.err_tol_force_acc;
   for(int i = 0; i <= p.nsofttypes; i++)
     w->soft[i] = p.force_softening[i];
-  if(p.periodic)
+  if(w->pm)
     {
       double rcut     = p.rcut;
       double asmth    = p.asmth;
@@ -338,7 +343,7 @@ int32_t gpugrav_destroy(gpugrav_ctx *c)
                         &c->depth_order, &c->w_sm, &c->w_cl, &c->w_link, &c->g_key, &c->g_key_alt, &c->g_val, &c->g_val_alt, &c->g_bfs, &c->g_np, &c->g_poff, &c->g_sm, &c->g_rel, &c->g_kids, &c->g_pm, &c->g_pst, &c->g_stack, &c->acc_s, &c->pot_s,
                         &c->nint_s, &c->oldacc_s, &c->oldacc_in, &c->out_acc, &c->out_pot, &c->out_nint, &c->scratch,
                         &c->g_groups, &c->g_ngroups, &c->g_gpd, &c->g_gseg, &c->g_gflag, &c->g_gid, &c->m_sys, &c->m_doms,
-                        &c->pm_pos, &c->pm_mass, &c->pm_acc, &c->pm_pot};
+                        &c->pm_pos, &c->pm_mass, &c->pm_acc, &c->pm_pot, &c->ewd, &c->ewd32};
   gg::pm_release(c);
   for(auto *b : bufs)
     b->release();
@@ -556,6 +561,25 @@ int32_t gpugrav_pm_periodic(gpugrav_ctx *c, int32_t pmgrid, int64_t n, const dou
   return GPUGRAV_OK;
 }
 
+int32_t gpugrav_set_ewald_table(gpugrav_ctx *c, int32_t en, const double *fx, const double *fy, const double *fz,
+                                const double *pot)
+{
+  if(!c)
+    return GPUGRAV_ERR_INVALID;
+  if(en != gg::kEwaldN || !fx || !fy || !fz || !pot)
+    return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_set_ewald_table: needs en = 64 and four tables");
+  const size_t m = (size_t)(en + 1) * (en + 1) * (en + 1);
+  std::vector<double> t(4 * m);
+  memcpy(t.data(), fx, m * sizeof(double));
+  memcpy(t.data() + m, fy, m * sizeof(double));
+  memcpy(t.data() + 2 * m, fz, m * sizeof(double));
+  memcpy(t.data() + 3 * m, pot, m * sizeof(double));
+  DeviceGuard g(c->device);
+  CK(cudaStreamSynchronize(c->stream), "Ewald tables");  // no walk may read the old tables
+  CK(gg::ewald_upload(c, t.data()), "Ewald tables");
+  return GPUGRAV_OK;
+}
+
 int32_t gpugrav_set_target_slice(gpugrav_ctx *c, int32_t slice, int32_t nslices)
 {
   if(!c)
@@ -584,6 +608,11 @@ int32_t gpugrav_walk(gpugrav_ctx *c, const float *oldacc, double *acc, double *p
     return fail(c, GPUGRAV_ERR_OOM, "gpugrav_walk: device allocation");
   WalkConst wc;
   make_walk_const(c->prm, &wc);
+  if(wc.ewald)
+    {
+      CK(gg::ewald_ensure(c), "Ewald tables");
+      wc.ewd = c->ewd.as<double>();
+    }
   c->want_pot = (pot != nullptr);
   CK(cudaMemcpyAsync(c->wconst.p, &wc, sizeof(wc), cudaMemcpyHostToDevice, st), "walk constants");
   cudaEventRecord(c->ev[7], st);
@@ -819,6 +848,13 @@ int32_t gpugrav_direct(gpugrav_ctx *c, int64_t ntargets, const int64_t *targets,
     return fail(c, GPUGRAV_ERR_OOM, "gpugrav_direct: allocation");
   WalkConst wc;
   make_walk_const(c->prm, &wc);
+  if(wc.ewald)
+    {
+      if(mode == GPUGRAV_DIRECT_CUT)
+        return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_direct: no Rcut without the TreePM split (asmth == 0)");
+      CK(gg::ewald_ensure(c), "Ewald tables");
+      wc.ewd = c->ewd.as<double>();
+    }
   CK(cudaMemcpyAsync(c->wconst.p, &wc, sizeof(wc), cudaMemcpyHostToDevice, st), "walk constants");
   CK(cudaMemcpyAsync(dt.p, targets, ntargets * 8, cudaMemcpyHostToDevice, st), "targets");
   CK(gg::direct_stage(c, wc, ntargets, dt.as<int64_t>(), mode == GPUGRAV_DIRECT_CUT, da.as<double>(), dp.as<double>()),

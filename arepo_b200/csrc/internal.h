@@ -50,9 +50,16 @@ struct BuildConst
 };
 
 // Walk constants
+constexpr int kEwaldN = 64;  // EN of the Ewald correction tables (src/gravity/forcetree.h:90)
+
 struct WalkConst
 {
-  int32_t periodic;
+  int32_t periodic;  // nearest-image separations
+  int32_t pm;        // TreePM split: Rcut prune and erfc table (periodic with Asmth > 0)
+  int32_t ewald;     // pure periodic tree: Ewald correction per interaction (periodic without PM)
+  int32_t pad0;
+  double ewd_fac_intp;       // 2 EN / L
+  const double *ewd;         // device tables fx | fy | fz | pot, (EN+1)^3 each
   int32_t bh;        // 1: Barnes-Hut criterion (ErrTolTheta > 0), 0: relative criterion
   double box, half_box;
   double theta;      // ErrTolTheta
@@ -62,6 +69,70 @@ struct WalkConst
   float tab_force[kNtab + 1];
   float tab_pot[kNtab + 1];
 };
+
+#ifdef __CUDACC__
+// Ewald correction force and potential for the separation (dx, dy, dz) = source - target: trilinear
+// interpolation of the octant tables with the sign flips of ewald_corr / ewald_pot_corr
+// (src/gravity/forcetree_ewald.c:268-391), same operations in the same order (FP64).
+__device__ __forceinline__ void ewald_corr(double dx, double dy, double dz, const WalkConst &w, double *fper, double &pcorr)
+{
+  constexpr int m = kEwaldN + 1;
+  const size_t total = (size_t)m * m * m;
+  int signx, signy, signz;
+  if(dx < 0)
+    {
+      dx    = -dx;
+      signx = +1;
+    }
+  else
+    signx = -1;
+  if(dy < 0)
+    {
+      dy    = -dy;
+      signy = +1;
+    }
+  else
+    signy = -1;
+  if(dz < 0)
+    {
+      dz    = -dz;
+      signz = +1;
+    }
+  else
+    signz = -1;
+  double u = dx * w.ewd_fac_intp;
+  int i    = (int)u;
+  if(i >= kEwaldN)
+    i = kEwaldN - 1;
+  u -= i;
+  double v = dy * w.ewd_fac_intp;
+  int j    = (int)v;
+  if(j >= kEwaldN)
+    j = kEwaldN - 1;
+  v -= j;
+  double ww = dz * w.ewd_fac_intp;
+  int k     = (int)ww;
+  if(k >= kEwaldN)
+    k = kEwaldN - 1;
+  ww -= k;
+  const double f1 = (1 - u) * (1 - v) * (1 - ww), f2 = (1 - u) * (1 - v) * (ww), f3 = (1 - u) * (v) * (1 - ww),
+               f4 = (1 - u) * (v) * (ww), f5 = (u) * (1 - v) * (1 - ww), f6 = (u) * (1 - v) * (ww), f7 = (u) * (v) * (1 - ww),
+               f8 = (u) * (v) * (ww);
+  const size_t b = ((size_t)i * m + j) * m + k;
+  double r[4];
+#pragma unroll
+  for(int c = 0; c < 4; c++)
+    {
+      const double *t = w.ewd + c * total;
+      r[c] = t[b] * f1 + t[b + 1] * f2 + t[b + m] * f3 + t[b + m + 1] * f4 + t[b + m * m] * f5 + t[b + m * m + 1] * f6 +
+             t[b + m * m + m] * f7 + t[b + m * m + m + 1] * f8;
+    }
+  fper[0] = signx * r[0];
+  fper[1] = signy * r[1];
+  fper[2] = signz * r[2];
+  pcorr   = r[3];
+}
+#endif
 
 // Device buffer that only grows.
 struct DevBuf
@@ -136,6 +207,10 @@ struct gpugrav_ctx
   gg::DevBuf g_groups, g_ngroups;             // walk groups (first, count, root, criterion), their count
   gg::DevBuf g_gpd, g_gseg, g_gflag, g_gid;   // group construction scratch
   int32_t slice = 0, nslices = 1;             // target slice of the walks (gpugrav_set_target_slice)
+  // Ewald correction tables (ewald.cu): FP64 and float4 copies, scaled to ewd_box (or the caller's)
+  gg::DevBuf ewd, ewd32;
+  double ewd_box = 0;
+  bool ewd_user  = false;
   // periodic PM long-range force (pm.cu): mesh size of the cuFFT plans, plans, meshes, particles
   int32_t pm_grid = 0, pm_plan_f = 0, pm_plan_b = 0;
   gg::DevBuf pm_rho, pm_rhok, pm_pos, pm_mass, pm_acc, pm_pot;
@@ -174,6 +249,9 @@ cudaError_t walk32_prepare(gpugrav_ctx *c, const WalkConst &wc);
 cudaError_t walk32_launch(gpugrav_ctx *c);
 cudaError_t groups_stage(gpugrav_ctx *c);
 cudaError_t slice_mask_stage(gpugrav_ctx *c, bool fp32);
+const std::vector<double> &ewald_unit_table();
+cudaError_t ewald_upload(gpugrav_ctx *c, const double *user);
+cudaError_t ewald_ensure(gpugrav_ctx *c);
 cudaError_t pm_stage(gpugrav_ctx *c, int pmgrid, int64_t np, const double *pos, const double *mass, double *acc, double *pot,
                      int *cufft_status);
 void pm_release(gpugrav_ctx *c);

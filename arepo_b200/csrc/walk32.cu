@@ -83,6 +83,9 @@ struct W32Const
   float soft[GPUGRAV_MAX_SOFTTYPES + 1];
   float2 tab[kNtab + 1];   // (f[i], f[i+1] - f[i]) of the force table
   float2 tabp[kNtab + 1];  // same for the potential table
+  const float4 *ewd;       // Ewald correction (fx, fy, fz, pot) per table entry (pure periodic tree)
+  float ewd_fac;           // 2 EN / L
+  int pad;
 };
 
 // ------------------------------------------------------------------------------
@@ -222,9 +225,35 @@ struct Tgt
   int ni;
 };
 
+// Ewald correction (force, potential) for the separation (dx, dy, dz) = source - target:
+// the trilinear interpolation and sign flips of ewald_corr (src/gravity/forcetree_ewald.c:268-342)
+// in FP32 on the float4 table.
+__device__ __forceinline__ float4 ewald_corr32(float dx, float dy, float dz, const W32Const &w)
+{
+  constexpr int m = kEwaldN + 1;
+  const float sx = dx < 0.0f ? 1.0f : -1.0f, sy = dy < 0.0f ? 1.0f : -1.0f, sz = dz < 0.0f ? 1.0f : -1.0f;
+  float u = fabsf(dx) * w.ewd_fac, v = fabsf(dy) * w.ewd_fac, s = fabsf(dz) * w.ewd_fac;
+  const int i = min((int)u, kEwaldN - 1), j = min((int)v, kEwaldN - 1), k = min((int)s, kEwaldN - 1);
+  u -= i;
+  v -= j;
+  s -= k;
+  const float4 *t = w.ewd + ((i * m + j) * m + k);
+  const float4 a0 = __ldg(t), a1 = __ldg(t + 1), a2 = __ldg(t + m), a3 = __ldg(t + m + 1);
+  const float4 b0 = __ldg(t + m * m), b1 = __ldg(t + m * m + 1), b2 = __ldg(t + m * m + m), b3 = __ldg(t + m * m + m + 1);
+  const float f1 = (1 - u) * (1 - v) * (1 - s), f2 = (1 - u) * (1 - v) * s, f3 = (1 - u) * v * (1 - s), f4 = (1 - u) * v * s;
+  const float f5 = u * (1 - v) * (1 - s), f6 = u * (1 - v) * s, f7 = u * v * (1 - s), f8 = u * v * s;
+  float4 r;
+  r.x = a0.x * f1 + a1.x * f2 + a2.x * f3 + a3.x * f4 + b0.x * f5 + b1.x * f6 + b2.x * f7 + b3.x * f8;
+  r.y = a0.y * f1 + a1.y * f2 + a2.y * f3 + a3.y * f4 + b0.y * f5 + b1.y * f6 + b2.y * f7 + b3.y * f8;
+  r.z = a0.z * f1 + a1.z * f2 + a2.z * f3 + a3.z * f4 + b0.z * f5 + b1.z * f6 + b2.z * f7 + b3.z * f8;
+  r.w = a0.w * f1 + a1.w * f2 + a2.w * f3 + a3.w * f4 + b0.w * f5 + b1.w * f6 + b2.w * f7 + b3.w * f8;
+  return make_float4(sx * r.x, sy * r.y, sz * r.z, r.w);
+}
+
 // One target against one list entry.  An entry beyond Rcut of this target (periodic) is
 // masked, not branched around; the softening branch is taken only inside the spline support.
-template <bool PERIODIC, bool POT>
+// EWALD: pure periodic tree (nearest image, no split), plus the Ewald correction of the entry.
+template <bool PERIODIC, bool POT, bool EWALD = false>
 __device__ __forceinline__ void interact(const float4 e, const float hj, Tgt &T, const W32Const &w)
 {
   const float dx   = e.x - T.x, dy = e.y - T.y, dz = e.z - T.z;
@@ -298,6 +327,15 @@ __device__ __forceinline__ void interact(const float4 e, const float hj, Tgt &T,
   T.az           = fmaf(dz, fm, T.az);
   if(POT)
     T.pot = fmaf(m, wp, T.pot);
+  if(EWALD)
+    {
+      const float4 c = ewald_corr32(dx, dy, dz, w);
+      T.ax           = fmaf(m, c.x, T.ax);
+      T.ay           = fmaf(m, c.y, T.ay);
+      T.az           = fmaf(m, c.z, T.az);
+      if(POT)
+        T.pot = fmaf(m, c.w, T.pot);
+    }
   T.ni += in ? 1 : 0;  // list entries all have mass != 0
 }
 
@@ -325,7 +363,7 @@ namespace
   while(0)
 #endif
 
-template <bool PERIODIC, bool POT, int TPL>
+template <bool PERIODIC, bool POT, int TPL, bool EWALD = false>
 __device__ __forceinline__ void evaluate(const float4 *__restrict__ LP, const float *__restrict__ LH, int nl, Tgt (&T)[TPL],
                                          const W32Const &w)
 {
@@ -336,7 +374,7 @@ __device__ __forceinline__ void evaluate(const float4 *__restrict__ LP, const fl
       const float hj = LH[j];
 #pragma unroll
       for(int k = 0; k < TPL; k++)
-        interact<PERIODIC, POT>(e, hj, T[k], w);
+        interact<PERIODIC, POT, EWALD>(e, hj, T[k], w);
     }
 #pragma unroll
   for(int k = 0; k < TPL; k++)
@@ -349,7 +387,7 @@ __device__ __forceinline__ void evaluate(const float4 *__restrict__ LP, const fl
     }
 }
 
-template <bool PERIODIC, bool POT, int TPL>
+template <bool PERIODIC, bool POT, int TPL, bool EWALD = false>
 __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const double4 *__restrict__ g_sm, const float4 *__restrict__ g_rel,
                                                         const int4 *__restrict__ g_kids, const double4 *__restrict__ g_pm,
                                                         const uint8_t *__restrict__ g_pst, const double4 *__restrict__ tpm,
@@ -564,7 +602,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
             {
               if(nl + 32 > kListCap)
                 {
-                  evaluate<PERIODIC, POT, TPL>(LP, LH, nl, T, w);
+                  evaluate<PERIODIC, POT, TPL, EWALD>(LP, LH, nl, T, w);
                   nl = 0;
                   __syncwarp();
                 }
@@ -624,7 +662,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
           if(nl >= kEvalAt)
             {
               WALK_STAT(0, nl);
-              evaluate<PERIODIC, POT, TPL>(LP, LH, nl, T, w);
+              evaluate<PERIODIC, POT, TPL, EWALD>(LP, LH, nl, T, w);
               nl = 0;
               __syncwarp();
             }
@@ -632,7 +670,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
       if(nl > 0)
         {
           WALK_STAT(0, nl);
-          evaluate<PERIODIC, POT, TPL>(LP, LH, nl, T, w);
+          evaluate<PERIODIC, POT, TPL, EWALD>(LP, LH, nl, T, w);
           __syncwarp();
         }
 #pragma unroll
@@ -799,6 +837,7 @@ void make_w32(const WalkConst &wc, W32Const *w)
   w->erracc    = (float)wc.erracc;
   w->periodic  = wc.periodic;
   w->bh        = wc.bh;
+  w->ewd_fac   = (float)wc.ewd_fac_intp;
   for(int i = 0; i <= GPUGRAV_MAX_SOFTTYPES; i++)
     w->soft[i] = (float)wc.soft[i];
   for(int i = 0; i <= kNtab; i++)
@@ -855,7 +894,8 @@ cudaError_t groups_stage(gpugrav_ctx *c)
 {
   const int64_t n = c->n;
   cudaStream_t st = c->stream;
-  const int cap   = 32 * ((c->walk32_tpl == 1 || c->multi) ? 1 : 2);
+  const bool ewald = c->prm.periodic && !(c->prm.asmth > 0);  // the Ewald variant walks one target per lane
+  const int cap    = 32 * ((c->walk32_tpl == 1 || c->multi || ewald) ? 1 : 2);
   GG_TRY(cudaMemsetAsync(c->g_ngroups.p, 0, sizeof(int), st));
   if(n == 0)
     return cudaSuccess;
@@ -932,19 +972,25 @@ cudaError_t walk32_prepare(gpugrav_ctx *c, const WalkConst &wc)
   cudaStream_t st = c->stream;
   W32Const w;
   make_w32(wc, &w);
+  if(wc.ewald)
+    {
+      GG_TRY(ewald_ensure(c));
+      w.ewd = c->ewd32.as<float4>();
+    }
   GG_TRY(c->scratch.ensure(sizeof(W32Const) + 256));
   GG_TRY(cudaMemcpyAsync(c->scratch.p, &w, sizeof(w), cudaMemcpyHostToDevice, st));
   GG_TRY(cudaStreamSynchronize(st));  // `w` lives on this stack frame
   int dev = 0, sms = 0, per_sm = 0;
   GG_TRY(cudaGetDevice(&dev));
   GG_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  const bool periodic = wc.periodic != 0;
+  const bool periodic = wc.pm != 0;  // TreePM split (Rcut, erfc table)
   const bool pot      = c->want_pot;
-  const int tpl       = (c->walk32_tpl == 1 || c->multi) ? 1 : 2;
-  Walk32Kernel kern = tpl == 2 ? (periodic ? (pot ? k_walk32<true, true, 2> : k_walk32<true, false, 2>)
-                                           : (pot ? k_walk32<false, true, 2> : k_walk32<false, false, 2>))
-                               : (periodic ? (pot ? k_walk32<true, true, 1> : k_walk32<true, false, 1>)
-                                           : (pot ? k_walk32<false, true, 1> : k_walk32<false, false, 1>));
+  const int tpl       = (c->walk32_tpl == 1 || c->multi || wc.ewald) ? 1 : 2;
+  Walk32Kernel kern = wc.ewald ? (pot ? k_walk32<false, true, 1, true> : k_walk32<false, false, 1, true>)
+                      : tpl == 2 ? (periodic ? (pot ? k_walk32<true, true, 2> : k_walk32<true, false, 2>)
+                                             : (pot ? k_walk32<false, true, 2> : k_walk32<false, false, 2>))
+                                 : (periodic ? (pot ? k_walk32<true, true, 1> : k_walk32<true, false, 1>)
+                                             : (pot ? k_walk32<false, true, 1> : k_walk32<false, false, 1>));
   GG_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * kWarps, 0));
   if(per_sm < 1)
     per_sm = 1;

@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk64(const double4 *__restric
           dz   = nearest(sm.z - pos_z, w);
           r2   = dx * dx + dy * dy + dz * dz;
           const double len = cl.w;
-          if(w.periodic && r2 > w.rcut2)
+          if(w.pm && r2 > w.rcut2)
             {
               double eff_dist = w.rcut + 0.5 * len;
               double dist     = nearest(cl.x - pos_x, w);
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk64(const double4 *__restric
         {
           double r            = sqrt(r2);
           double factor_force = 0, factor_pot = 0;
-          if(w.periodic)
+          if(w.pm)
             {
               double tabentry = w.asmthfac * r;
               int tabindex    = (int)tabentry;
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk64(const double4 *__restric
             {
               double rinv  = 1.0 / r;
               double rinv3 = rinv * rinv * rinv;
-              if(w.periodic)
+              if(w.pm)
                 {
                   fac = rinv3 + rinv * factor_force * w.asmthinv2;
                   wp  = rinv * factor_pot;
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk64(const double4 *__restric
                   fac       = h3_inv * (SF8 + SF9 * u + SF10 * u2 + SF11 * u3 + SF12 / u3);
                   wp        = h_inv * (SF13 + SF14 / u + u2 * (SF1 + u * (SF15 + u * (SF16 + SF17 * u))));
                 }
-              if(w.periodic && r > 0)
+              if(w.pm && r > 0)
                 {
                   double rinv = 1.0 / r;
                   fac += rinv * factor_force * w.asmthinv2;
@@ -237,6 +237,16 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk64(const double4 *__restric
           acc_x += dx * fac;
           acc_y += dy * fac;
           acc_z += dz * fac;
+          if(w.ewald)
+            {
+              // all further periodic images, src/gravity/forcetree_walk.c:469-477
+              double fcorr[3], pcorr;
+              ewald_corr(dx, dy, dz, w, fcorr, pcorr);
+              acc_x += mass * fcorr[0];
+              acc_y += mass * fcorr[1];
+              acc_z += mass * fcorr[2];
+              pot += mass * pcorr;
+            }
           ninteractions++;
         }
     }

@@ -76,6 +76,12 @@ class GravityTree:
                                                  L.ptr(pos), L.ptr(mass), L.ptr(acc), L.ptr(pot), mem))
         return acc, pot
 
+    def set_ewald_table(self, fx, fy, fz, pot):
+        """AREPO's Ewald correction tables (Ewd_fcorrx/y/z, Ewd_potcorr after ewald_init: scaled to
+        the box), (65, 65, 65) or flat doubles each, for a periodic context without PM (asmth = 0)."""
+        arrs = [np.ascontiguousarray(a, np.float64).ravel() for a in (fx, fy, fz, pot)]
+        self._check(self.lib.gpugrav_set_ewald_table(self._ctx, 64, *[L.ptr(a) for a in arrs]))
+
     def set_target_slice(self, slice_: int, nslices: int):
         """Walk only slice `slice_` of `nslices` key-ordered target slices; other targets' outputs
         are zero (the slices of G ranks sum to the full result)."""

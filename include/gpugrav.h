@@ -184,6 +184,17 @@ int32_t gpugrav_walk(gpugrav_ctx *ctx, const float *oldacc, double *acc, double 
  * sum exactly to the unsliced result. Default 0 of 1 (all targets). */
 int32_t gpugrav_set_target_slice(gpugrav_ctx *ctx, int32_t slice, int32_t nslices);
 
+/* Periodic box without PM (params: periodic = 1, asmth = 0): the walks use the nearest image of
+ * every node and particle plus the reference's Ewald correction per interaction
+ * (src/gravity/forcetree_walk.c:469-477, forcetree_ewald.c:268-391). The correction tables are those
+ * of ewald_init (forcetree_ewald.c:89-254): by default the library computes them on the host on
+ * first use (the reference's sums, bit-identical; a few seconds, once per process) and scales them
+ * to box_size; a caller that already holds AREPO's tables (Ewd_fcorrx/y/z, Ewd_potcorr after
+ * ewald_init, i.e. scaled to its box) passes them here: en = EN = 64, (en+1)^3 doubles each,
+ * last index fastest. They are copied; they stay in use until the next call. */
+int32_t gpugrav_set_ewald_table(gpugrav_ctx *ctx, int32_t en, const double *fcorrx, const double *fcorry,
+                                const double *fcorrz, const double *potcorr);
+
 /* Long-range periodic PM accelerations (without G) and potentials of n particles; replaces
  * pmforce_periodic(0, NULL) (src/gravity/pm/pm_periodic.c:1572-1936): CIC assignment on a
  * pmgrid^3 mesh, FFT, Green's function -exp(-k^2 Asmth^2)/k^2 with the CIC deconvolution, inverse

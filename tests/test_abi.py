@@ -57,7 +57,9 @@ int main(void){
 
 def test_invalid_params_rejected_before_gpu_work(lib):
     ctx = C.c_void_p()
-    p = L.make_params(periodic=True, asmth=0.0, rcut=0.0)  # periodic needs Asmth, Rcut > 0
+    p = L.make_params(periodic=True, asmth=0.01, rcut=0.0)  # the TreePM split needs Rcut > 0
+    assert lib.gpugrav_create(C.byref(ctx), 0, C.byref(p)) == L.ERR_INVALID
+    p = L.make_params(periodic=True, asmth=-0.01, rcut=0.04)  # Asmth < 0 (0 selects the Ewald-corrected tree)
     assert lib.gpugrav_create(C.byref(ctx), 0, C.byref(p)) == L.ERR_INVALID
     p = L.make_params(periodic=False)
     p.abi_version = 99
