@@ -37,6 +37,7 @@ MEM_HOST = 0
 MEM_DEVICE = 1
 PREC_FP64 = 0
 PREC_FP32 = 1
+FLAG_MULTIPLE_NODE_SOFTENING = 1
 DIRECT_FULL = 0
 DIRECT_CUT = 1
 
@@ -57,6 +58,8 @@ class Params(C.Structure):
         ("top_node_factor", C.c_double),
         ("multiple_domains", C.c_int32),
         ("precision", C.c_int32),
+        ("flags", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -165,6 +168,7 @@ _SIGS = {
     "gpugrav_set_target_slice": (C.c_int32, [_P, C.c_int32, C.c_int32]),
     "gpugrav_pm_periodic": (C.c_int32, [_P, C.c_int32, C.c_int64, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_set_ewald_table": (C.c_int32, [_P, C.c_int32, _P, _P, _P, _P]),
+    "gpugrav_export_mass_per_type": (C.c_int32, [_P, _P]),
     "gpugrav_compute": (C.c_int32, [_P, C.c_int64, _P, _P, _P, _P, C.POINTER(Domain), _P, C.c_int32, _P, _P, _P, C.c_int32]),
     "gpugrav_get_domain": (C.c_int32, [_P, C.POINTER(Domain)]),
     "gpugrav_get_order": (C.c_int32, [_P, _P]),
@@ -233,6 +237,7 @@ def make_params(
     top_node_factor: float = 2.5,
     multiple_domains: int = 8,
     precision: int = PREC_FP64,
+    multiple_node_softening: bool = False,
 ) -> Params:
     """softening: Plummer-equivalent epsilon per softening type. The spline support is
     ForceSoftening = 2.8 * epsilon with a trailing zero entry (set_softenings,
@@ -254,6 +259,7 @@ def make_params(
     p.top_node_factor = top_node_factor
     p.multiple_domains = multiple_domains
     p.precision = precision
+    p.flags = FLAG_MULTIPLE_NODE_SOFTENING if multiple_node_softening else 0
     return p
 
 

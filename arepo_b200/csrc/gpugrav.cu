@@ -143,6 +143,8 @@ int validate_params(const gpugrav_params *p)
     return GPUGRAV_ERR_INVALID;
   if(p->multiple_domains < 1 || p->multiple_domains > 512 || !(p->top_node_factor > 0))
     return GPUGRAV_ERR_INVALID;
+  if((p->flags & ~GPUGRAV_FLAG_MULTIPLE_NODE_SOFTENING) != 0 || p->reserved != 0)
+    return GPUGRAV_ERR_INVALID;
   return GPUGRAV_OK;
 }
 
@@ -207,6 +209,8 @@ void gg::make_walk_const(const gpugrav_params &p, WalkConst *w)
 {
   memset(w, 0, sizeof(*w));
   w->periodic = p.periodic;
+  w->mns      = (p.flags & GPUGRAV_FLAG_MULTIPLE_NODE_SOFTENING) ? 1 : 0;
+  w->nsoft    = p.nsofttypes;
   w->pm       = p.periodic && p.asmth > 0;
   w->ewald    = p.periodic && !(p.asmth > 0);
   if(w->ewald)
@@ -343,7 +347,8 @@ int32_t gpugrav_destroy(gpugrav_ctx *c)
                         &c->depth_order, &c->w_sm, &c->w_cl, &c->w_link, &c->g_key, &c->g_key_alt, &c->g_val, &c->g_val_alt, &c->g_bfs, &c->g_np, &c->g_poff, &c->g_sm, &c->g_rel, &c->g_kids, &c->g_pm, &c->g_pst, &c->g_stack, &c->acc_s, &c->pot_s,
                         &c->nint_s, &c->oldacc_s, &c->oldacc_in, &c->out_acc, &c->out_pot, &c->out_nint, &c->scratch,
                         &c->g_groups, &c->g_ngroups, &c->g_gpd, &c->g_gseg, &c->g_gflag, &c->g_gid, &c->m_sys, &c->m_doms,
-                        &c->pm_pos, &c->pm_mass, &c->pm_acc, &c->pm_pot, &c->ewd, &c->ewd32};
+                        &c->pm_pos, &c->pm_mass, &c->pm_acc, &c->pm_pot, &c->ewd, &c->ewd32, &c->n_mpt, &c->w_mpt,
+                        &c->g_mpt};
   gg::pm_release(c);
   for(auto *b : bufs)
     b->release();
@@ -435,6 +440,7 @@ int32_t gpugrav_load(gpugrav_ctx *c, int64_t n, const double *pos, const double 
   bc.n        = n;
   bc.periodic = c->prm.periodic;
   bc.nsoft    = c->prm.nsofttypes;
+  bc.mns      = (c->prm.flags & GPUGRAV_FLAG_MULTIPLE_NODE_SOFTENING) ? 1 : 0;
   bc.box      = c->prm.box_size;
   for(int i = 0; i <= c->prm.nsofttypes; i++)
     bc.soft[i] = c->prm.force_softening[i];
@@ -561,6 +567,22 @@ int32_t gpugrav_pm_periodic(gpugrav_ctx *c, int32_t pmgrid, int64_t n, const dou
   return GPUGRAV_OK;
 }
 
+int32_t gpugrav_export_mass_per_type(gpugrav_ctx *c, double *out)
+{
+  if(!c || !out)
+    return GPUGRAV_ERR_INVALID;
+  if(!c->built)
+    return fail(c, GPUGRAV_ERR_STATE, "gpugrav_export_mass_per_type before gpugrav_build");
+  if(!(c->prm.flags & GPUGRAV_FLAG_MULTIPLE_NODE_SOFTENING))
+    return fail(c, GPUGRAV_ERR_STATE, "gpugrav_export_mass_per_type: built without MULTIPLE_NODE_SOFTENING");
+  DeviceGuard g(c->device);
+  CK(cudaMemcpyAsync(out, c->n_mpt.p, (size_t)c->num_nodes * c->prm.nsofttypes * sizeof(double), cudaMemcpyDeviceToHost,
+                     c->stream),
+     "download per-type masses");
+  CK(cudaStreamSynchronize(c->stream), "download per-type masses");
+  return GPUGRAV_OK;
+}
+
 int32_t gpugrav_set_ewald_table(gpugrav_ctx *c, int32_t en, const double *fx, const double *fy, const double *fz,
                                 const double *pot)
 {
@@ -613,6 +635,8 @@ int32_t gpugrav_walk(gpugrav_ctx *c, const float *oldacc, double *acc, double *p
       CK(gg::ewald_ensure(c), "Ewald tables");
       wc.ewd = c->ewd.as<double>();
     }
+  if(wc.mns)
+    wc.w_mpt = c->w_mpt.as<double>();
   c->want_pot = (pot != nullptr);
   CK(cudaMemcpyAsync(c->wconst.p, &wc, sizeof(wc), cudaMemcpyHostToDevice, st), "walk constants");
   cudaEventRecord(c->ev[7], st);

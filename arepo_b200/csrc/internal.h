@@ -45,6 +45,8 @@ struct BuildConst
   int32_t nleaves;   // NTopleaves
   int32_t periodic;
   int32_t nsoft;
+  int32_t mns;       // MULTIPLE_NODE_SOFTENING: per-type node masses
+  int32_t pad;
   double box;
   double soft[GPUGRAV_MAX_SOFTTYPES + 1];
 };
@@ -57,7 +59,10 @@ struct WalkConst
   int32_t periodic;  // nearest-image separations
   int32_t pm;        // TreePM split: Rcut prune and erfc table (periodic with Asmth > 0)
   int32_t ewald;     // pure periodic tree: Ewald correction per interaction (periodic without PM)
+  int32_t mns;       // MULTIPLE_NODE_SOFTENING: nodes used per softening type
+  int32_t nsoft;
   int32_t pad0;
+  const double *w_mpt;  // FP64 walk: per-type masses of each walk entry (nodes), nsoft each
   double ewd_fac_intp;       // 2 EN / L
   const double *ewd;         // device tables fx | fy | fz | pot, (EN+1)^3 each
   int32_t bh;        // 1: Barnes-Hut criterion (ErrTolTheta > 0), 0: relative criterion
@@ -195,6 +200,7 @@ struct gpugrav_ctx
   gg::DevBuf cnt, base, hcnt, hack_list, hack_scratch, counters;
   gg::DevBuf top, skel;                       // top nodes, skeleton description
   gg::DevBuf n_suns, n_depth, n_cl, n_sm, n_maxsoft, n_size, n_father, n_sibling, n_next, n_dfs, n_first;
+  gg::DevBuf n_mpt, w_mpt, g_mpt;             // MULTIPLE_NODE_SOFTENING: per-type node masses (node, walk, FP32 layouts)
   gg::DevBuf p_next, p_father, p_dfs;
   gg::DevBuf depth_hist, depth_order;
   gg::DevBuf w_sm, w_cl, w_link;              // walk layout (DFS order)

@@ -843,12 +843,37 @@ __global__ void k_depth_scatter(const uint8_t *__restrict__ depth, int64_t nn, i
 __global__ void k_moments(const int32_t *__restrict__ order, int count, int64_t n, const int32_t *__restrict__ suns,
                           const double4 *__restrict__ pm, const uint8_t *__restrict__ st, const double4 *__restrict__ cl,
                           double4 *__restrict__ sm, uint8_t *__restrict__ maxsoft, int32_t *__restrict__ size,
-                          const BuildConst *__restrict__ bc)
+                          const BuildConst *__restrict__ bc, double *__restrict__ mpt)
 {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if(t >= count)
     return;
   int64_t k = order[t];
+  if(mpt)
+    {
+      // ExtNodes[].mass_per_type (MULTIPLE_NODE_SOFTENING, src/gravity/forcetree.c:1256-1308): per type,
+      // the particle masses and the child sums of slots 0..7 in order
+      const int ns = bc->nsoft;
+      double acc[GPUGRAV_MAX_SOFTTYPES];
+      for(int q = 0; q < ns; q++)
+        acc[q] = 0.0;
+      for(int q = 0; q < 8; q++)
+        {
+          int32_t c = suns[8 * k + q];
+          if(c < 0)
+            continue;
+          if(c < n)
+            {
+              const int s = st[c];
+              acc[s]      = __dadd_rn(acc[s], pm[c].w);
+            }
+          else
+            for(int u = 0; u < ns; u++)
+              acc[u] = __dadd_rn(acc[u], mpt[(c - n) * ns + u]);
+        }
+      for(int q = 0; q < ns; q++)
+        mpt[k * ns + q] = acc[q];
+    }
   double mass = 0, sx = 0, sy = 0, sz = 0;
   int ms      = bc->nsoft;  // NSOFTTYPES + NSOFTTYPES_HYDRO: the entry whose softening is 0
   int sz_     = 1;
@@ -967,7 +992,8 @@ __global__ void k_layout(int64_t n, int64_t nn, const double4 *__restrict__ pm, 
                          const int32_t *__restrict__ pdfs, const double4 *__restrict__ sm, const double4 *__restrict__ cl,
                          const uint8_t *__restrict__ maxsoft, const int32_t *__restrict__ size,
                          const int32_t *__restrict__ ndfs, double4 *__restrict__ w_sm, double4 *__restrict__ w_cl,
-                         int2 *__restrict__ w_link, int *err)
+                         int2 *__restrict__ w_link, int *err, const double *__restrict__ mpt, int nsoft,
+                         double *__restrict__ w_mpt)
 {
   const int64_t ne = n + nn;
   for(int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n + nn; t += (int64_t)gridDim.x * blockDim.x)
@@ -996,6 +1022,9 @@ __global__ void k_layout(int64_t n, int64_t nn, const double4 *__restrict__ pm, 
           w_sm[e]   = sm[k];
           w_cl[e]   = cl[k];
           w_link[e] = make_int2(e + size[k], (int)maxsoft[k] | kNodeFlag);
+          if(w_mpt)
+            for(int q = 0; q < nsoft; q++)
+              w_mpt[(int64_t)e * nsoft + q] = mpt[k * nsoft + q];
         }
     }
 }
@@ -1299,8 +1328,12 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
   launches += 2;
 
   c->mark("b5 depth buckets");
-  // 6. moments bottom-up
+  // 6. moments bottom-up (with MULTIPLE_NODE_SOFTENING also the per-type masses)
   const int32_t *order = c->depth_order.as<int32_t>();
+  const bool mns       = (c->prm.flags & GPUGRAV_FLAG_MULTIPLE_NODE_SOFTENING) != 0;
+  const int nsoft      = c->prm.nsofttypes;
+  if(mns)
+    GG_TRY(c->n_mpt.ensure((size_t)(nn + 16) * nsoft * sizeof(double)));
   for(int d = maxd; d >= 0; d--)
     {
       int cnt = h_hist[d];
@@ -1309,7 +1342,7 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
       k_moments<<<(cnt + 127) / 128, 128, 0, st>>>(order + h_off[d], cnt, n, c->n_suns.as<int32_t>(), c->s_pm.as<double4>(),
                                                    c->s_st.as<uint8_t>(), c->n_cl.as<double4>(), c->n_sm.as<double4>(),
                                                    c->n_maxsoft.as<uint8_t>(), c->n_size.as<int32_t>(),
-                                                   c->bconst.as<BuildConst>());
+                                                   c->bconst.as<BuildConst>(), mns ? c->n_mpt.as<double>() : nullptr);
       launches++;
     }
   c->mark("b6 moments");
@@ -1348,10 +1381,14 @@ cudaError_t build_stage(gpugrav_ctx *c, int *status)
       GG_TRY(c->w_sm.ensure(ne * sizeof(double4)));
       GG_TRY(c->w_cl.ensure(ne * sizeof(double4)));
       GG_TRY(c->w_link.ensure(ne * sizeof(int2)));
+      if(mns)
+        GG_TRY(c->w_mpt.ensure((size_t)ne * nsoft * sizeof(double)));
       k_layout<<<grid_for(ne, 256), 256, 0, st>>>(n, nn, c->s_pm.as<double4>(), c->s_st.as<uint8_t>(), c->p_dfs.as<int32_t>(),
                                                    c->n_sm.as<double4>(), c->n_cl.as<double4>(), c->n_maxsoft.as<uint8_t>(),
                                                    c->n_size.as<int32_t>(), c->n_dfs.as<int32_t>(), c->w_sm.as<double4>(),
-                                                   c->w_cl.as<double4>(), c->w_link.as<int2>(), a.err);
+                                                   c->w_cl.as<double4>(), c->w_link.as<int2>(), a.err,
+                                                   mns ? c->n_mpt.as<double>() : nullptr, nsoft,
+                                                   mns ? c->w_mpt.as<double>() : nullptr);
       launches++;
     }
   c->mark("b8 layout64");

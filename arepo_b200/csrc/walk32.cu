@@ -85,7 +85,10 @@ struct W32Const
   float2 tabp[kNtab + 1];  // same for the potential table
   const float4 *ewd;       // Ewald correction (fx, fy, fz, pot) per table entry (pure periodic tree)
   float ewd_fac;           // 2 EN / L
-  int pad;
+  int mns;                 // MULTIPLE_NODE_SOFTENING: nodes used per softening type
+  const float *mpt;        // per-type node masses, breadth-first order, nsoft each
+  int nsoft;
+  int pad2;
 };
 
 // ------------------------------------------------------------------------------
@@ -122,7 +125,8 @@ __global__ void k_g_fill(int64_t nn, int64_t n, const int32_t *__restrict__ sort
                          const int32_t *__restrict__ bfs, const int32_t *__restrict__ poff, const double4 *__restrict__ sm,
                          const double4 *__restrict__ cl, const uint8_t *__restrict__ maxsoft, const double4 *__restrict__ pm,
                          const uint8_t *__restrict__ st, double4 *__restrict__ g_sm, float4 *__restrict__ g_rel,
-                         int4 *__restrict__ g_kids, double4 *__restrict__ g_pm, uint8_t *__restrict__ g_pst, int *err)
+                         int4 *__restrict__ g_kids, double4 *__restrict__ g_pm, uint8_t *__restrict__ g_pst, int *err,
+                         const double *__restrict__ mpt, int nsoft, float *__restrict__ g_mpt)
 {
   for(int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < nn; b += (int64_t)gridDim.x * blockDim.x)
     {
@@ -154,6 +158,9 @@ __global__ void k_g_fill(int64_t nn, int64_t n, const int32_t *__restrict__ sort
             }
         }
       g_kids[b] = make_int4(fc, fp, nc | (npc << 4), (int)maxsoft[k]);
+      if(g_mpt)
+        for(int q = 0; q < nsoft; q++)
+          g_mpt[b * nsoft + q] = (float)mpt[(int64_t)k * nsoft + q];
     }
 }
 
@@ -491,6 +498,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
           float hj     = 0;
           int fc = 0, fp = 0, nc = 0, np = 0;
           bool vote = false, vote_keep = false;  // per-target vote pending; entry kept if accepted
+          bool split = false;                    // MULTIPLE_NODE_SOFTENING: accepted node listed per type
           float4 vrel = make_float4(0, 0, 0, 0);   // centre - CoM, side of a voting node
           if(node >= 0)
             {
@@ -522,8 +530,15 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                       else
                         open = (L2 > rmin2 * 1.44f) || (m * L2 > rmin2 * rmin2 * aold_min) ||
                                (fabsf(cx) < 0.6f * L + ex && fabsf(cy) < 0.6f * L + ey && fabsf(cz) < 0.6f * L + ez);
-                      if(!open && hj > h_min && rmin2 < hj * hj)
-                        open = true;
+                      if(!open && hj > h_min)
+                        {
+                          // a target's softening is below the node's largest: open inside that
+                          // softening, or (MULTIPLE_NODE_SOFTENING) use the node per softening type
+                          if(w.mns)
+                            split = true;
+                          else if(rmin2 < hj * hj)
+                            open = true;
+                        }
                       if(open)
                         {
                           action = 2;
@@ -571,7 +586,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                           o = (L2 > r2 * 1.44f) || (entry.w * L2 > r2 * r2 * ta) ||
                               (fabsf(entry.x + vrel.x - tx) < 0.6f * L && fabsf(entry.y + vrel.y - ty) < 0.6f * L &&
                                fabsf(entry.z + vrel.z - tz) < 0.6f * L);
-                        if(!o && hj > th && r2 < hj * hj)
+                        if(!o && !w.mns && hj > th && r2 < hj * hj)
                           o = true;
                         need = o;
                       }
@@ -579,18 +594,41 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
               if(vote && !need)
                 {
                   action = vote_keep ? 1 : 0;
+                  split  = w.mns && hj > h_min;
                   nc = np = 0;
                 }
             }
-          // accepted nodes -> list
-          const unsigned am = __ballot_sync(0xffffffffu, action == 1);
-          if(action == 1)
+          // accepted nodes -> list (nodes used per softening type follow below)
+          const unsigned am = __ballot_sync(0xffffffffu, action == 1 && !split);
+          if(action == 1 && !split)
             {
               const int pos = nl + __popc(am & lt_mask);
               LP[pos]       = entry;
               LH[pos]       = hj;
             }
           nl += __popc(am);
+          // MULTIPLE_NODE_SOFTENING: one entry per softening type with that type's mass and softening
+          // (forcetree_walk.c:382-401); for a target whose own softening exceeds the node's largest
+          // this equals the single entry, the kernel being linear in the mass
+          if(__ballot_sync(0xffffffffu, action == 1 && split))
+            for(int t = 0; t < w.nsoft; t++)
+              {
+                if(nl + 32 > kListCap)
+                  {
+                    evaluate<PERIODIC, POT, TPL, EWALD>(LP, LH, nl, T, w);
+                    nl = 0;
+                    __syncwarp();
+                  }
+                const float mt    = (action == 1 && split) ? w.mpt[(int64_t)node * w.nsoft + t] : 0.0f;
+                const unsigned km = __ballot_sync(0xffffffffu, mt != 0.0f);
+                if(mt != 0.0f)
+                  {
+                    const int pos = nl + __popc(km & lt_mask);
+                    LP[pos]       = make_float4(entry.x, entry.y, entry.z, mt);
+                    LH[pos]       = w.soft[t];
+                  }
+                nl += __popc(km);
+              }
           // particles of opened nodes -> list, one particle per lane per round; particles beyond
           // Rcut of the whole group are dropped
           const int npx  = (action == 2) ? np : 0;
@@ -838,6 +876,8 @@ void make_w32(const WalkConst &wc, W32Const *w)
   w->periodic  = wc.periodic;
   w->bh        = wc.bh;
   w->ewd_fac   = (float)wc.ewd_fac_intp;
+  w->mns       = wc.mns;
+  w->nsoft     = wc.nsoft;
   for(int i = 0; i <= GPUGRAV_MAX_SOFTTYPES; i++)
     w->soft[i] = (float)wc.soft[i];
   for(int i = 0; i <= kNtab; i++)
@@ -927,6 +967,9 @@ cudaError_t layout32_stage(gpugrav_ctx *c)
   const int64_t n = c->n, nn = c->num_nodes;
   cudaStream_t st = c->stream;
   GG_TRY(layout32_buffers(c, n, nn));
+  const bool mns = (c->prm.flags & GPUGRAV_FLAG_MULTIPLE_NODE_SOFTENING) != 0;
+  if(mns)
+    GG_TRY(c->g_mpt.ensure((size_t)(nn + 16) * c->prm.nsofttypes * sizeof(float)));
   k_g_keys<<<grid_for(nn, 256), 256, 0, st>>>(nn, c->n_depth.as<uint8_t>(), c->n_dfs.as<int32_t>(), c->g_key.as<uint64_t>(),
                                                c->g_val.as<int32_t>());
   size_t tb = 0;
@@ -947,7 +990,9 @@ cudaError_t layout32_stage(gpugrav_ctx *c)
                                                c->g_poff.as<int32_t>(), c->n_sm.as<double4>(), c->n_cl.as<double4>(),
                                                c->n_maxsoft.as<uint8_t>(), c->s_pm.as<double4>(), c->s_st.as<uint8_t>(),
                                                c->g_sm.as<double4>(), c->g_rel.as<float4>(), c->g_kids.as<int4>(),
-                                               c->g_pm.as<double4>(), c->g_pst.as<uint8_t>(), err);
+                                               c->g_pm.as<double4>(), c->g_pst.as<uint8_t>(), err,
+                                               mns ? c->n_mpt.as<double>() : nullptr, c->prm.nsofttypes,
+                                               mns ? c->g_mpt.as<float>() : nullptr);
   GG_TRY(cudaGetLastError());
   int e = 0;
   GG_TRY(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -977,6 +1022,8 @@ cudaError_t walk32_prepare(gpugrav_ctx *c, const WalkConst &wc)
       GG_TRY(ewald_ensure(c));
       w.ewd = c->ewd32.as<float4>();
     }
+  if(wc.mns)
+    w.mpt = c->g_mpt.as<float>();
   GG_TRY(c->scratch.ensure(sizeof(W32Const) + 256));
   GG_TRY(cudaMemcpyAsync(c->scratch.p, &w, sizeof(w), cudaMemcpyHostToDevice, st));
   GG_TRY(cudaStreamSynchronize(st));  // `w` lives on this stack frame

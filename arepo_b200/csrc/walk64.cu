@@ -91,6 +91,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk64(const double4 *__restric
         continue;
 
       double dx, dy, dz, r2, mass, hmax;
+      bool split = false;  // MULTIPLE_NODE_SOFTENING: node used per softening type
       if(!node)
         {
           // single particle, src/gravity/forcetree_walk.c:178-195
@@ -164,7 +165,9 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk64(const double4 *__restric
           double h_j = w.soft[link.y & 0xff];
           if(h_j > h_i)
             {
-              if(r2 < h_j * h_j)
+              if(w.mns)
+                split = true;  // src/gravity/forcetree_walk.c:296-308
+              else if(r2 < h_j * h_j)
                 {
                   next = i + 1;
                   continue;
@@ -191,61 +194,74 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk64(const double4 *__restric
               factor_force     = (1.0 - tabweight) * w.tab_force[tabindex] + tabweight * w.tab_force[tabindex + 1];
               factor_pot       = (1.0 - tabweight) * w.tab_pot[tabindex] + tabweight * w.tab_pot[tabindex + 1];
             }
-          double fac, wp;
-          if(r >= hmax)
+          // per softening type under MULTIPLE_NODE_SOFTENING (forcetree_walk.c:382-401), else once
+          const int t0 = split ? 0 : -1, t1 = split ? w.nsoft : 0;
+          for(int type = t0; type < t1; type++)
             {
-              double rinv  = 1.0 / r;
-              double rinv3 = rinv * rinv * rinv;
-              if(w.pm)
+              if(type >= 0)
                 {
-                  fac = rinv3 + rinv * factor_force * w.asmthinv2;
-                  wp  = rinv * factor_pot;
+                  mass             = w.w_mpt[(int64_t)i * w.nsoft + type];
+                  const double hjt = w.soft[type];
+                  hmax             = (hjt > h_i) ? hjt : h_i;
+                }
+              if(!mass)
+                continue;
+              double fac, wp;
+              if(r >= hmax)
+                {
+                  double rinv  = 1.0 / r;
+                  double rinv3 = rinv * rinv * rinv;
+                  if(w.pm)
+                    {
+                      fac = rinv3 + rinv * factor_force * w.asmthinv2;
+                      wp  = rinv * factor_pot;
+                    }
+                  else
+                    {
+                      fac = rinv3;
+                      wp  = -rinv;
+                    }
                 }
               else
                 {
-                  fac = rinv3;
-                  wp  = -rinv;
+                  double h_inv  = 1.0 / hmax;
+                  double h3_inv = h_inv * h_inv * h_inv;
+                  double u      = r * h_inv;
+                  if(u < 0.5)
+                    {
+                      double u2 = u * u;
+                      fac       = h3_inv * (SF1 + u2 * (SF2 * u + SF3));
+                      wp        = h_inv * (SF4 + u2 * (SF5 + u2 * (SF6 * u + SF7)));
+                    }
+                  else
+                    {
+                      double u2 = u * u;
+                      double u3 = u2 * u;
+                      fac       = h3_inv * (SF8 + SF9 * u + SF10 * u2 + SF11 * u3 + SF12 / u3);
+                      wp        = h_inv * (SF13 + SF14 / u + u2 * (SF1 + u * (SF15 + u * (SF16 + SF17 * u))));
+                    }
+                  if(w.pm && r > 0)
+                    {
+                      double rinv = 1.0 / r;
+                      fac += rinv * factor_force * w.asmthinv2;
+                      wp += rinv * (factor_pot + 1.0);
+                    }
                 }
-            }
-          else
-            {
-              double h_inv  = 1.0 / hmax;
-              double h3_inv = h_inv * h_inv * h_inv;
-              double u      = r * h_inv;
-              if(u < 0.5)
+              pot += mass * wp;
+              fac *= mass;
+              acc_x += dx * fac;
+              acc_y += dy * fac;
+              acc_z += dz * fac;
+              if(w.ewald)
                 {
-                  double u2 = u * u;
-                  fac       = h3_inv * (SF1 + u2 * (SF2 * u + SF3));
-                  wp        = h_inv * (SF4 + u2 * (SF5 + u2 * (SF6 * u + SF7)));
+                  // all further periodic images, src/gravity/forcetree_walk.c:469-477
+                  double fcorr[3], pcorr;
+                  ewald_corr(dx, dy, dz, w, fcorr, pcorr);
+                  acc_x += mass * fcorr[0];
+                  acc_y += mass * fcorr[1];
+                  acc_z += mass * fcorr[2];
+                  pot += mass * pcorr;
                 }
-              else
-                {
-                  double u2 = u * u;
-                  double u3 = u2 * u;
-                  fac       = h3_inv * (SF8 + SF9 * u + SF10 * u2 + SF11 * u3 + SF12 / u3);
-                  wp        = h_inv * (SF13 + SF14 / u + u2 * (SF1 + u * (SF15 + u * (SF16 + SF17 * u))));
-                }
-              if(w.pm && r > 0)
-                {
-                  double rinv = 1.0 / r;
-                  fac += rinv * factor_force * w.asmthinv2;
-                  wp += rinv * (factor_pot + 1.0);
-                }
-            }
-          pot += mass * wp;
-          fac *= mass;
-          acc_x += dx * fac;
-          acc_y += dy * fac;
-          acc_z += dz * fac;
-          if(w.ewald)
-            {
-              // all further periodic images, src/gravity/forcetree_walk.c:469-477
-              double fcorr[3], pcorr;
-              ewald_corr(dx, dy, dz, w, fcorr, pcorr);
-              acc_x += mass * fcorr[0];
-              acc_y += mass * fcorr[1];
-              acc_z += mass * fcorr[2];
-              pot += mass * pcorr;
             }
           ninteractions++;
         }

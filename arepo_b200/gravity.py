@@ -76,6 +76,12 @@ class GravityTree:
                                                  L.ptr(pos), L.ptr(mass), L.ptr(acc), L.ptr(pot), mem))
         return acc, pot
 
+    def mass_per_type(self) -> np.ndarray:
+        """ExtNodes[].mass_per_type of the last build (MULTIPLE_NODE_SOFTENING), reference node order."""
+        out = np.empty((self.tree_info().num_nodes, self.params.nsofttypes))
+        self._check(self.lib.gpugrav_export_mass_per_type(self._ctx, L.ptr(out)))
+        return out
+
     def set_ewald_table(self, fx, fy, fz, pot):
         """AREPO's Ewald correction tables (Ewd_fcorrx/y/z, Ewd_potcorr after ewald_init: scaled to
         the box), (65, 65, 65) or flat doubles each, for a periodic context without PM (asmth = 0)."""

@@ -70,7 +70,8 @@ enum
 typedef struct gpugrav_params
 {
   int32_t abi_version;                 /* GPUGRAV_ABI_VERSION */
-  int32_t periodic;                    /* 1: periodic box, TreePM short-range force (PMGRID builds);
+  int32_t periodic;                    /* 1: periodic box: TreePM short-range force (PMGRID builds) if asmth > 0,
+                                          Ewald-corrected tree (periodic builds without PMGRID) if asmth == 0;
                                           0: isolated, plain Newtonian tree (GRAVITY_NOT_PERIODIC, no PMGRID) */
   double box_size;                     /* All.BoxSize */
   double asmth;                        /* All.Asmth[0] (periodic only) */
@@ -85,7 +86,18 @@ typedef struct gpugrav_params
   double top_node_factor;              /* All.TopNodeFactor (library-built top tree only) */
   int32_t multiple_domains;            /* All.MultipleDomains (library-built top tree only) */
   int32_t precision;                   /* GPUGRAV_PREC_* */
+  int32_t flags;                       /* GPUGRAV_FLAG_* */
+  int32_t reserved;                    /* 0 */
 } gpugrav_params;
+
+/* gpugrav_params.flags */
+enum
+{
+  /* MULTIPLE_NODE_SOFTENING: a node whose largest softening exceeds the target's is used once per
+   * softening type with that type's mass (ExtNodes[].mass_per_type) instead of being opened
+   * (src/gravity/forcetree_walk.c:296-308, 382-401; src/gravity/forcetree.c:1222-1308) */
+  GPUGRAV_FLAG_MULTIPLE_NODE_SOFTENING = 1
+};
 
 /* Domain geometry: the globals set by domain_findExtent (src/domain/domain_box.c:169-196). */
 typedef struct gpugrav_domain
@@ -192,6 +204,10 @@ int32_t gpugrav_set_target_slice(gpugrav_ctx *ctx, int32_t slice, int32_t nslice
  * to box_size; a caller that already holds AREPO's tables (Ewd_fcorrx/y/z, Ewd_potcorr after
  * ewald_init, i.e. scaled to its box) passes them here: en = EN = 64, (en+1)^3 doubles each,
  * last index fastest. They are copied; they stay in use until the next call. */
+/* Read-back of ExtNodes[].mass_per_type under MULTIPLE_NODE_SOFTENING: num_nodes x nsofttypes
+ * doubles in the reference's node order (parity checks). */
+int32_t gpugrav_export_mass_per_type(gpugrav_ctx *ctx, double *out);
+
 int32_t gpugrav_set_ewald_table(gpugrav_ctx *ctx, int32_t en, const double *fcorrx, const double *fcorry,
                                 const double *fcorrz, const double *potcorr);
 

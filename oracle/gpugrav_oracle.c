@@ -71,7 +71,7 @@ typedef struct
   double erracc;     /* All.ErrTolForceAcc */
   double tnf;        /* All.TopNodeFactor */
   int mdom;          /* All.MultipleDomains */
-  int pad;
+  int flags;         /* bit 0: MULTIPLE_NODE_SOFTENING */
   double soft[16];   /* All.ForceSoftening[] */
 } or_params;
 
@@ -703,6 +703,35 @@ static void update_node(or_tree *t, int64_t no, int64_t sib, int64_t father, int
     }
 }
 
+/* ExtNodes[].mass_per_type of MULTIPLE_NODE_SOFTENING (force_update_node_recursive,
+ * src/gravity/forcetree.c:1222-1308): per node and softening type, the masses of the particles in
+ * slots 0..7 and the sums of the child nodes, in slot order.  Child nodes are created after their
+ * parents (higher index), so one pass from the last node to the root sees every child first.
+ * Returns 0, or -1 if that order does not hold. */
+int or_mass_per_type(int64_t num_nodes, const int32_t *suns, int64_t max_part, const double *mass, const uint8_t *stype,
+                     int nsoft, double *mpt)
+{
+  memset(mpt, 0, sizeof(double) * num_nodes * nsoft);
+  for(int64_t k = num_nodes - 1; k >= 0; k--)
+    for(int j = 0; j < 8; j++)
+      {
+        int64_t p = suns[8 * k + j];
+        if(p < 0)
+          continue;
+        if(p < max_part)
+          mpt[k * nsoft + stype[p]] += mass[p];
+        else
+          {
+            int64_t q = p - max_part;
+            if(q <= k)
+              return -1;
+            for(int t = 0; t < nsoft; t++)
+              mpt[k * nsoft + t] += mpt[q * nsoft + t];
+          }
+      }
+  return 0;
+}
+
 /*
  * Build the tree over particles given in insertion order.
  * max_part: index of the root (the reference uses All.MaxPart); max_nodes: capacity.
@@ -993,8 +1022,9 @@ void or_walk(int64_t ntargets, const int64_t *targets, const double *tpos, const
              const double *pos, const double *mass, const uint8_t *stype, const int32_t *p_next, int64_t max_part,
              int64_t num_nodes, const double *center, const double *len, const double *s, const double *nmass,
              const int32_t *sibling, const int32_t *nextnode, const uint8_t *maxsoft, const or_params *p, double *acc_out,
-             double *pot_out, int32_t *ninter_out)
+             double *pot_out, int32_t *ninter_out, const double *mpt)
 {
+  const int mns = (p->flags & 1) && mpt; /* MULTIPLE_NODE_SOFTENING */
   float tab_f[OR_NTAB + 1], tab_p[OR_NTAB + 1];
   const int pm    = p->periodic && p->asmth > 0;  /* TreePM split */
   const int ewald = p->periodic && !pm;           /* pure tree, Ewald-corrected */
@@ -1019,6 +1049,7 @@ void or_walk(int64_t ntargets, const int64_t *targets, const double *tpos, const
       while(no >= 0)
         {
           double dx, dy, dz, r2, m, hmax;
+          int64_t split = -1; /* node whose per-type masses are used (MULTIPLE_NODE_SOFTENING) */
           if(no < max_part)
             {
               dx = nearest(pos[3 * no + 0] - pos_x, p);
@@ -1092,7 +1123,9 @@ void or_walk(int64_t ntargets, const int64_t *targets, const double *tpos, const
               double h_j = p->soft[maxsoft[k]];
               if(h_j > h_i)
                 {
-                  if(r2 < h_j * h_j)
+                  if(mns)
+                    split = k; /* used per softening type instead of opened (forcetree_walk.c:296-308) */
+                  else if(r2 < h_j * h_j)
                     {
                       no = nextnode[k];
                       continue;
@@ -1118,6 +1151,18 @@ void or_walk(int64_t ntargets, const int64_t *targets, const double *tpos, const
                   factor_force     = (1.0 - tabweight) * tab_f[tabindex] + tabweight * tab_f[tabindex + 1];
                   factor_pot       = (1.0 - tabweight) * tab_p[tabindex] + tabweight * tab_p[tabindex + 1];
                 }
+              const int t0 = split >= 0 ? 0 : -1, t1 = split >= 0 ? p->nsoft : 0;
+              for(int type = t0; type < t1; type++)
+                {
+              double mm = m;
+              if(type >= 0)
+                {
+                  mm         = mpt[split * p->nsoft + type];
+                  double hjt = p->soft[type];
+                  hmax       = (hjt > h_i) ? hjt : h_i;
+                }
+              if(!mm)
+                continue;
               double fac, wp;
               if(r >= hmax)
                 {
@@ -1159,8 +1204,8 @@ void or_walk(int64_t ntargets, const int64_t *targets, const double *tpos, const
                       wp += rinv * (factor_pot + 1.0);
                     }
                 }
-              pot += m * wp;
-              fac *= m;
+              pot += mm * wp;
+              fac *= mm;
               acc_x += dx * fac;
               acc_y += dy * fac;
               acc_z += dz * fac;
@@ -1168,10 +1213,11 @@ void or_walk(int64_t ntargets, const int64_t *targets, const double *tpos, const
                 {
                   double fcorr[3], pcorr;
                   or_ewald_corr(dx, dy, dz, fcorr, &pcorr);
-                  acc_x += m * fcorr[0];
-                  acc_y += m * fcorr[1];
-                  acc_z += m * fcorr[2];
-                  pot += m * pcorr;
+                  acc_x += mm * fcorr[0];
+                  acc_y += mm * fcorr[1];
+                  acc_z += mm * fcorr[2];
+                  pot += mm * pcorr;
+                }
                 }
               ninteractions++;
             }

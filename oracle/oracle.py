@@ -55,7 +55,7 @@ class OrParams(C.Structure):
         ("erracc", C.c_double),
         ("tnf", C.c_double),
         ("mdom", C.c_int),
-        ("pad", C.c_int),
+        ("flags", C.c_int),  # bit 0: MULTIPLE_NODE_SOFTENING
         ("soft", C.c_double * MAX_SOFT),
     ]
 
@@ -111,7 +111,9 @@ def lib():
         _lib.or_build.argtypes = [i64, p, p, p, p, p, p, p, C.c_int, i64, i64] + [p] * 11 + [p]
         _lib.or_build.restype = i64
         _lib.or_shortrange_table.argtypes = [C.c_double, p, p]
-        _lib.or_walk.argtypes = [i64, p, p, p, p, p, p, p, p, i64, i64, p, p, p, p, p, p, p, p, p, p, p]
+        _lib.or_walk.argtypes = [i64, p, p, p, p, p, p, p, p, i64, i64, p, p, p, p, p, p, p, p, p, p, p, p]
+        _lib.or_mass_per_type.argtypes = [i64, p, i64, p, p, C.c_int, p]
+        _lib.or_mass_per_type.restype = C.c_int
         _lib.or_direct.argtypes = [i64, p, i64, p, p, p, p, p, p]
         _lib.or_ewald_table.argtypes = [p, p, p, p]
         _lib.or_set_ewald_table.argtypes = [C.c_double, p, p, p, p]
@@ -170,6 +172,7 @@ def make_params(
     softening=(0.01, 0.01),
     mdom: int = 8,
     tnf: float = 2.5,
+    mns: bool = False,
 ) -> OrParams:
     """softening: Plummer-equivalent epsilon per type; ForceSoftening = 2.8*eps (set_softenings,
     src/gravity/grav_softening.c:92-95) with a trailing zero entry."""
@@ -184,6 +187,7 @@ def make_params(
     p.erracc = erracc
     p.tnf = tnf
     p.mdom = mdom
+    p.flags = 1 if mns else 0
     for i, e in enumerate(softening):
         p.soft[i] = 2.8 * e
     p.soft[len(softening)] = 0.0
@@ -280,13 +284,27 @@ def walk(tree, pos_sorted, mass_sorted, st_sorted, oldacc_sorted, prm, targets=N
     mass_sorted = np.ascontiguousarray(mass_sorted, np.float64)
     st_sorted = np.ascontiguousarray(st_sorted, np.uint8)
     oldacc_sorted = np.ascontiguousarray(oldacc_sorted, np.float32)
+    mpt = None
+    if prm.flags & 1:
+        mpt = mass_per_type(tree, mass_sorted, st_sorted, prm)
     lib().or_walk(
         nt, _ptr(tg), _ptr(pos_sorted), _ptr(oldacc_sorted), _ptr(st_sorted), _ptr(pos_sorted), _ptr(mass_sorted),
         _ptr(st_sorted), _ptr(tree["p_next"]), tree["max_part"], tree["num_nodes"], _ptr(tree["center"]),
         _ptr(tree["len"]), _ptr(tree["s"]), _ptr(tree["mass"]), _ptr(tree["sibling"]), _ptr(tree["nextnode"]),
-        _ptr(tree["maxsoft"]), C.byref(prm), _ptr(acc), _ptr(pot), _ptr(ninter),
+        _ptr(tree["maxsoft"]), C.byref(prm), _ptr(acc), _ptr(pot), _ptr(ninter), _ptr(mpt),
     )
     return acc, pot, ninter
+
+
+def mass_per_type(tree, mass_sorted, st_sorted, prm):
+    """Per-node masses per softening type (MULTIPLE_NODE_SOFTENING's ExtNodes[].mass_per_type)."""
+    nn = tree["num_nodes"]
+    out = np.zeros((nn, prm.nsoft))
+    suns = np.ascontiguousarray(tree["suns"], np.int32)
+    if lib().or_mass_per_type(nn, _ptr(suns), tree["max_part"], _ptr(np.ascontiguousarray(mass_sorted, np.float64)),
+                              _ptr(np.ascontiguousarray(st_sorted, np.uint8)), prm.nsoft, _ptr(out)) != 0:
+        raise RuntimeError("child node created before its parent")
+    return out
 
 
 def direct(pos, mass, st, prm, targets):
@@ -387,6 +405,8 @@ def read_output(path):
         i = np.frombuffer(out["node_i32"], np.int32).reshape(-1, 4)
         r["node_center"], r["node_len"], r["node_s"], r["node_mass"] = f[:, 0:3], f[:, 3], f[:, 4:7], f[:, 7]
         r["node_sibling"], r["node_nextnode"], r["node_father"], r["node_maxsoft"] = i[:, 0], i[:, 1], i[:, 2], i[:, 3]
+        if "node_mpt" in out:
+            r["node_mpt"] = np.frombuffer(out["node_mpt"], np.float64).reshape(len(f), -1)
         r["p_next"] = np.frombuffer(out["nextnode"], np.int32)
         r["p_father"] = np.frombuffer(out["father"], np.int32)
     for ps in range(4):
@@ -404,11 +424,14 @@ def read_output(path):
 
 def run_ref(pos, mass, st, periodic, *, box=1.0, asmth=None, rcut=None, theta=0.7, erracc=0.0025,
             softening=(0.01, 0.01), mdom=8, tnf=2.5, passes=2, dump=1, gt=1, first=0, count=None, stride=1,
-            timeout=3600, ewald=False, ewald_table_out=None):
+            timeout=3600, ewald=False, ewald_table_out=None, mns=False):
     """Run the compiled reference harness; returns the parsed dump.  ewald=True: the periodic
     pure-tree build (no PM, Ewald correction); its table file is cached in oracle/_ref/ewald_cache
     (the reference writes it to the working directory), ewald_table_out dumps the scaled table."""
-    exe = os.path.join(REF_DIR, "ref_harness_ewald" if ewald else ("ref_harness_pm" if periodic else "ref_harness_iso"))
+    if mns and not (periodic and not ewald):
+        raise ValueError("the MULTIPLE_NODE_SOFTENING harness is a periodic TreePM build")
+    exe = os.path.join(REF_DIR, "ref_harness_ewald" if ewald else
+                       ("ref_harness_pm_mns" if mns else ("ref_harness_pm" if periodic else "ref_harness_iso")))
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
     cwd = None

@@ -133,6 +133,11 @@ static void dump_tree(FILE *f)
       int32_t v[4] = {Nodes[no].u.d.sibling, Nodes[no].u.d.nextnode, Nodes[no].u.d.father, Nodes[no].u.d.maxsofttype};
       wr(f, v, 4, 4);
     }
+#ifdef MULTIPLE_NODE_SOFTENING
+  wsec(f, "node_mpt", (int64_t)nn * NSOFTTYPES * 8);
+  for(int no = Tree_MaxPart; no < Tree_MaxPart + nn; no++)
+    wr(f, ExtNodes[no].mass_per_type, 8, NSOFTTYPES);
+#endif
   wsec(f, "nextnode", (int64_t)NumPart * 4);
   wr(f, Nextnode, 4, NumPart);
   wsec(f, "father", (int64_t)NumPart * 4);

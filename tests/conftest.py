@@ -16,7 +16,7 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-GOLDEN_CASES = ["grid16_pm", "hernquist2048_iso", "mix1500_pm", "grid12_ewald"]
+GOLDEN_CASES = ["grid16_pm", "hernquist2048_iso", "mix1500_pm", "grid12_ewald", "mns2000_pm"]
 
 
 def pytest_configure(config):

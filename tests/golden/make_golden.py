@@ -56,6 +56,17 @@ def cases():
     a = 1.25 / 64
     c["mix1500_pm"] = dict(pos=pos, mass=mass, softtype=st, softening=(0.001, 0.0003), periodic=True, box=1.0, asmth=a,
                            rcut=4.5 * a)
+    # MULTIPLE_NODE_SOFTENING: heavy particles with a large softening around a clump of light ones with
+    # a small softening, so that nodes whose largest softening exceeds the target's are common
+    rng = np.random.default_rng(1007)
+    n = 2000
+    st = (np.arange(n) >= 800).astype(np.uint8)
+    pos = np.where(st[:, None] == 0, np.mod(0.5 + 0.08 * rng.normal(size=(n, 3)), 1.0),
+                   np.mod(0.5 + 0.03 * rng.normal(size=(n, 3)), 1.0))
+    mass = np.where(st == 0, 8.0, 1.0) / n
+    a = 1.25 / 64
+    c["mns2000_pm"] = dict(pos=pos, mass=mass, softtype=st, softening=(0.01, 0.0008), periodic=True, box=1.0, asmth=a,
+                           rcut=4.5 * a, mns=True)
     # periodic pure tree with Ewald correction: 12^3 grid + displacements in a box of size 2
     g = ics.grid_box(n1=12, seed=1006, pmgrid=32)
     c["grid12_ewald"] = dict(pos=2.0 * g["pos"], mass=g["mass"], softtype=g["softtype"],
@@ -80,15 +91,16 @@ def main():
             continue
         soft = tuple(ic["softening"]) + (ic["softening"][-1],) * (2 - len(ic["softening"]))
         ewald = bool(ic.get("ewald", False))
+        mns = bool(ic.get("mns", False))
         tabf = tempfile.mktemp(suffix=".bin") if ewald else None
         ref = O.run_ref(ic["pos"], ic["mass"], ic["softtype"], ic["periodic"], box=ic["box"], asmth=ic["asmth"],
                         rcut=ic["rcut"], theta=0.7, erracc=0.0025, softening=soft, mdom=8, tnf=2.5, ewald=ewald,
-                        ewald_table_out=tabf)
+                        ewald_table_out=tabf, mns=mns)
         n = len(ic["mass"])
         m = ref["tree_meta"]
         mp = m["max_part"]
         prm = dict(periodic=bool(ic["periodic"]), box=ic["box"], asmth=ic["asmth"], rcut=ic["rcut"], rcut_cells=4.5,
-                   softening=list(soft), theta=0.7, erracc=0.0025, mdom=8, tnf=2.5, ewald=ewald)
+                   softening=list(soft), theta=0.7, erracc=0.0025, mdom=8, tnf=2.5, ewald=ewald, mns=mns)
         out = dict(
             params=np.array(json.dumps(prm)),
             pos=ic["pos"], mass=ic["mass"], softtype=ic["softtype"],
@@ -99,6 +111,8 @@ def main():
             node_nextnode=remap(ref["node_nextnode"], mp, n), node_father=remap(ref["node_father"], mp, n),
             p_next=remap(ref["p_next"], mp, n), p_father=remap(ref["p_father"], mp, n),
         )
+        if mns:
+            out["node_mpt"] = ref["node_mpt"]
         if ewald:
             raw = open(tabf, "rb").read()
             os.remove(tabf)

@@ -112,3 +112,32 @@ def test_fp32_walk_isolated_outliers_stay_local(cuda_lib):
     rel64, glob64 = _err(a64[tg], d)
     rel32, glob32 = _err(a32[tg], d)
     assert glob32 <= glob64 * 1.02 + 2e-5, (glob32, glob64)
+
+
+def test_fp32_walk_multiple_node_softening(cuda_lib):
+    """MULTIPLE_NODE_SOFTENING with two very different softenings: nodes with large-softening mass
+    near small-softening targets are listed per type in the FP32 walk; its error against the direct
+    sum is no larger than the FP64 parity walk's (which follows the reference per target)."""
+    rng = np.random.default_rng(41)
+    n = 40000
+    st = (np.arange(n) >= n // 3).astype(np.uint8)
+    pos = np.where(st[:, None] == 0, np.mod(0.5 + 0.08 * rng.normal(size=(n, 3)), 1.0),
+                   np.mod(0.5 + 0.03 * rng.normal(size=(n, 3)), 1.0))
+    mass = np.where(st == 0, 8.0, 1.0) / n
+    a = 1.25 / 128
+    ic = dict(pos=pos, mass=mass, softtype=st, softening=(0.004, 0.0004), periodic=True, box=1.0, asmth=a,
+              rcut=4.5 * a)
+    tg = np.sort(rng.choice(n, 2048, replace=False))
+    out = {}
+    for prec in (L.PREC_FP64, L.PREC_FP32):
+        prm = ics.params_for(ic, precision=prec)
+        prm.flags = L.FLAG_MULTIPLE_NODE_SOFTENING
+        with GravityTree(prm) as t:
+            acc, _, ni, _ = t.compute_grav_accelerations(pos, mass, st)
+            d, _ = t.direct(tg, cut=True)
+        out[prec] = (acc, ni, d)
+    d = out[L.PREC_FP64][2]
+    rel64, glob64 = _err(out[L.PREC_FP64][0][tg], d)
+    rel32, glob32 = _err(out[L.PREC_FP32][0][tg], d)
+    assert glob32 <= glob64 * 1.02 + 2e-5, (glob32, glob64)
+    assert rel32 <= rel64 * 1.02 + 2e-5, (rel32, rel64)

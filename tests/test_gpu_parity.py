@@ -21,12 +21,13 @@ def gpu_params(p, precision=L.PREC_FP64):
     return L.make_params(periodic=p["periodic"], box_size=p["box"], asmth=p["asmth"], rcut=p["rcut"],
                          rcut_cells=p["rcut_cells"], softening=tuple(p["softening"]), err_tol_theta=p["theta"],
                          err_tol_force_acc=p["erracc"], top_node_factor=p["tnf"], multiple_domains=p["mdom"],
-                         precision=precision)
+                         precision=precision, multiple_node_softening=p.get("mns", False))
 
 
 def oracle_params(p):
     return O.make_params(p["periodic"], box=p["box"], asmth=p["asmth"], rcut=p["rcut"], rcut_cells=p["rcut_cells"],
-                         theta=p["theta"], erracc=p["erracc"], softening=tuple(p["softening"]), mdom=p["mdom"], tnf=p["tnf"])
+                         theta=p["theta"], erracc=p["erracc"], softening=tuple(p["softening"]), mdom=p["mdom"], tnf=p["tnf"],
+                         mns=p.get("mns", False))
 
 
 def top_equal(a, b):
@@ -70,6 +71,8 @@ def test_tree_bitexact_with_reference_topnodes(name, cuda_lib):
         t.domain_decomposition(g["pos"], g["mass"], g["softtype"])
         t.construct_forcetree(topnodes=g["top"])
         assert_tree_equal(t.export_tree(), g)
+        if "node_mpt" in g:  # MULTIPLE_NODE_SOFTENING: ExtNodes[].mass_per_type
+            assert np.array_equal(t.mass_per_type(), g["node_mpt"])
 
 
 @pytest.mark.parametrize("name", GOLDEN_CASES)

@@ -10,7 +10,8 @@ from oracle import oracle as O
 def oracle_params(g):
     p = g["params"]
     return O.make_params(p["periodic"], box=p["box"], asmth=p["asmth"], rcut=p["rcut"], rcut_cells=p["rcut_cells"],
-                         theta=p["theta"], erracc=p["erracc"], softening=tuple(p["softening"]), mdom=p["mdom"], tnf=p["tnf"])
+                         theta=p["theta"], erracc=p["erracc"], softening=tuple(p["softening"]), mdom=p["mdom"], tnf=p["tnf"],
+                         mns=p.get("mns", False))
 
 
 def top_equal(a, b):
@@ -40,6 +41,8 @@ def test_oracle_matches_reference(name):
                       ("maxsoft", "node_maxsoft"), ("sibling", "node_sibling"), ("nextnode", "node_nextnode"),
                       ("father", "node_father"), ("p_next", "p_next"), ("p_father", "p_father")):
         assert np.array_equal(t[k_or], g[k_g]), k_or
+    if "node_mpt" in g:
+        assert np.array_equal(O.mass_per_type(t, out["mass_sorted"], out["st_sorted"], prm), g["node_mpt"])
     for ps in range(2):
         assert np.array_equal(out[f"acc{ps}"], g[f"acc{ps}"])
         assert np.array_equal(out[f"pot{ps}"], g[f"pot{ps}"])
