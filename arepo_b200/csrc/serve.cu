@@ -423,6 +423,8 @@ cudaError_t serve_reserve(gpugrav_serve *s)
   GG_TRY(gg::build_reserve(c, n, n, nsys));
   GG_TRY(gg::layout32_reserve(c, n, n));
   GG_TRY(s->up.ensure((size_t)n * (7 * sizeof(double) + 1)));
+  // pinned staging of the result downloads: requests up to 2^20 particles without a later allocation
+  GG_TRY(s->staging.ensure((size_t)(n < (1 << 20) ? n : (1 << 20)) * 9 * sizeof(double)));
   return s->dl.ensure((size_t)n * 9 * sizeof(double));
 }
 
@@ -918,13 +920,18 @@ int32_t gpugrav_serve_poll(gpugrav_serve *s, int64_t *id, int64_t *n, double *po
                                                       s->acc.as<double4>(), s->dl.as<double>());
       const size_t b = (size_t)r->n * 3 * sizeof(double);
       SCK(cudaGetLastError(), "download");
-      if(pos)
-        SCK(cudaMemcpyAsync(pos, d, b, cudaMemcpyDeviceToHost, st), "download");
-      if(vel)
-        SCK(cudaMemcpyAsync(vel, d + 3 * r->n, b, cudaMemcpyDeviceToHost, st), "download");
-      if(acc)
-        SCK(cudaMemcpyAsync(acc, d + 6 * r->n, b, cudaMemcpyDeviceToHost, st), "download");
+      // one DMA into pinned staging, then host copies (a device-to-pageable copy is several times slower)
+      if(s->staging.ensure(3 * b) != cudaSuccess)
+        return sfail(s, GPUGRAV_ERR_OOM, "download staging");
+      SCK(cudaMemcpyAsync(s->staging.p, d, 3 * b, cudaMemcpyDeviceToHost, st), "download");
       SCK(cudaStreamSynchronize(st), "download");
+      const char *h = (const char *)s->staging.p;
+      if(pos)
+        memcpy(pos, h, b);
+      if(vel)
+        memcpy(vel, h + b, b);
+      if(acc)
+        memcpy(acc, h + 2 * b, b);
     }
   pool_free(s, r->pool_off, r->n);
   if(times)

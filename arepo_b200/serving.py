@@ -98,26 +98,36 @@ class GravityServer:
         st = self.stats()
         return st.waiting > 0 or st.running > 0
 
-    def poll(self) -> ServeResult | None:
+    def poll(self, out=None) -> ServeResult | None:
+        """Oldest finished request, or None.  `out` (optional): a mapping from request id to
+        caller-owned (pos, vel, acc) float64 arrays of shape (n, 3) that receive the result (no
+        allocation per result); ids not in it get new arrays."""
         rid, n = C.c_int64(), C.c_int64()
         self._check(self.lib.gpugrav_serve_poll(self._srv, C.byref(rid), C.byref(n), None, None, None, 0, None))
         if rid.value < 0:
             return None
-        pos = np.empty((n.value, 3))
-        vel = np.empty((n.value, 3))
-        acc = np.empty((n.value, 3))
+        bufs = out.get(int(rid.value)) if out is not None else None
+        if bufs is not None:
+            pos, vel, acc = bufs
+            for a in bufs:
+                if a.shape != (n.value, 3) or a.dtype != np.float64 or not a.flags.c_contiguous:
+                    raise ValueError("result buffers must be C-contiguous float64 of shape (n, 3)")
+        else:
+            pos = np.empty((n.value, 3))
+            vel = np.empty((n.value, 3))
+            acc = np.empty((n.value, 3))
         times = np.empty(3)
         self._check(self.lib.gpugrav_serve_poll(self._srv, C.byref(rid), C.byref(n), L.ptr(pos), L.ptr(vel), L.ptr(acc),
                                                 n.value, L.ptr(times)))
         return ServeResult(int(rid.value), pos, vel, acc, float(times[0]), float(times[1]), float(times[2]))
 
-    def poll_all(self) -> list[ServeResult]:
-        out = []
+    def poll_all(self, out=None) -> list[ServeResult]:
+        res = []
         while True:
-            r = self.poll()
+            r = self.poll(out)
             if r is None:
-                return out
-            out.append(r)
+                return res
+            res.append(r)
 
     def run_to_completion(self) -> dict[int, ServeResult]:
         res = {}

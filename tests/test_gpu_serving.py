@@ -63,6 +63,26 @@ def test_served_force_matches_direct_sum(kind, cuda_lib):
     assert np.percentile(e, 99) < 2e-2
 
 
+def test_poll_into_caller_buffers(cuda_lib):
+    prm = serving_params(EPS)
+    sysa = _system("plummer", 3000, 61)
+    with GravityServer(prm, max_systems=4, max_particles=1 << 16) as srv:
+        srv.submit(1, *sysa, nsteps=2, dt=0.005)
+        ref = srv.run_to_completion()[1]
+    with GravityServer(prm, max_systems=4, max_particles=1 << 16) as srv:
+        srv.submit(1, *sysa, nsteps=2, dt=0.005)
+        bufs = {1: tuple(np.full((3000, 3), np.nan) for _ in range(3))}
+        got = None
+        for _ in range(50):  # 4 ticks are needed
+            srv.tick()
+            for r in srv.poll_all(bufs):
+                got = r
+            if got is not None:
+                break
+    assert got.pos is bufs[1][0] and got.acc is bufs[1][2]
+    assert np.array_equal(got.pos, ref.pos) and np.array_equal(got.vel, ref.vel) and np.array_equal(got.acc, ref.acc)
+
+
 def test_kick_drift_kick_matches_numpy_leapfrog(cuda_lib):
     """Same KDK sequence in numpy with the served force replaced by FP64 direct summation: the
     trajectories differ only by the tree's force error over a few steps."""
