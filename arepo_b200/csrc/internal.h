@@ -219,7 +219,7 @@ struct gpugrav_ctx
   bool ewd_user  = false;
   // periodic PM long-range force (pm.cu): mesh size of the cuFFT plans, plans, meshes, particles
   int32_t pm_grid = 0, pm_plan_f = 0, pm_plan_b = 0;
-  gg::DevBuf pm_rho, pm_rhok, pm_pos, pm_mass, pm_acc, pm_pot;
+  gg::DevBuf pm_rho, pm_rhok, pm_pos, pm_mass, pm_acc, pm_pot, pm_tab;
   int group_slack = 99;                       // group cuts between cells (< 64) or key order only (GPUGRAV_GROUP_SLACK)
   bool layout32_valid = false;
   // several independent systems in one build (serving): system of each sorted particle, domain of

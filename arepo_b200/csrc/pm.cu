@@ -6,7 +6,8 @@
 //      1-dx and dx, periodic, :1090-1165), FP64 atomics;
 //   2. real-to-complex FFT (cuFFT, FP64);
 //   3. Green's function -exp(-k^2 Asmth^2) / k^2 times the CIC deconvolution
-//      (sin(k d/2) / (k d/2))^-4 per axis, zero mode cleared (:1620-1704);
+//      (sin(k d/2) / (k d/2))^-4 per axis, zero mode cleared (:1620-1704); both factors separate
+//      into per-axis tables;
 //   4. complex-to-real FFT: the potential mesh (unnormalised, as the FFTW backward transform);
 //   5. per particle, the 4-point finite difference of the potential,
 //      fac ((4/3)(phi[-1] - phi[+1]) - (1/6)(phi[-2] - phi[+2])), fac = 4 pi G / L^3 / (2 d)
@@ -20,6 +21,7 @@
 #include <cufft.h>
 
 #include <cmath>
+#include <vector>
 
 #include "internal.h"
 
@@ -72,16 +74,11 @@ __global__ void k_pm_deposit(int64_t np, const double *__restrict__ pos, const d
     }
 }
 
-__device__ __forceinline__ double deconv_axis(double k, double dhalf)
-{
-  if(k == 0.0)
-    return 1.0;
-  const double a = k * dhalf;
-  return sin(a) / a;
-}
 
-// mesh of the forward transform: n x n x (n/2 + 1), last index fastest
-__global__ void k_pm_green(int n, double kfac, double asmth2, double dhalf, cufftDoubleComplex *__restrict__ rk)
+// mesh of the forward transform: n x n x (n/2 + 1), last index fastest.  The Gaussian and the CIC
+// deconvolution factor per axis: tab[i] = (exp(-k_i^2 Asmth^2), 1 / sinc(k_i d / 2)^4) for the wave
+// number k_i of mesh index i, so that an entry costs one product and one division.
+__global__ void k_pm_green(int n, double kfac, const double2 *__restrict__ tab, cufftDoubleComplex *__restrict__ rk)
 {
   const int nz      = n / 2 + 1;
   const int64_t tot = (int64_t)n * n * nz;
@@ -96,8 +93,8 @@ __global__ void k_pm_green(int n, double kfac, double asmth2, double dhalf, cuff
       double g        = 0.0;  // the zero mode carries the mean density: no force
       if(k2 > 0)
         {
-          const double ff = 1.0 / (deconv_axis(kx, dhalf) * deconv_axis(ky, dhalf) * deconv_axis(kz, dhalf));
-          g               = -exp(-k2 * asmth2) / k2 * (ff * ff * ff * ff);
+          const double2 a = tab[x], b = tab[y], c = tab[z];
+          g               = -(a.x * b.x * c.x) * (a.y * b.y * c.y) / k2;
         }
       rk[i].x *= g;
       rk[i].y *= g;
@@ -192,6 +189,27 @@ cudaError_t pm_stage(gpugrav_ctx *c, int pmgrid, int64_t np, const double *pos, 
     }
   GG_TRY(c->pm_rho.ensure(N3 * sizeof(double)));
   GG_TRY(c->pm_rhok.ensure(NC * sizeof(cufftDoubleComplex)));
+  {
+    // per-axis factors of the Green's function (host, n entries)
+    const double bx = c->prm.box_size, dd = bx / n, kf = 2.0 * M_PI / bx, a2 = c->prm.asmth * c->prm.asmth;
+    std::vector<double2> tab(n);
+    for(int i = 0; i < n; i++)
+      {
+        const int ii   = i >= n / 2 ? i - n : i;
+        const double k = kf * ii;
+        double s       = 1.0;
+        if(ii != 0)
+          {
+            const double a = k * 0.5 * dd;
+            s              = sin(a) / a;
+          }
+        const double f = 1.0 / s;
+        tab[i]         = make_double2(exp(-k * k * a2), f * f * f * f);
+      }
+    GG_TRY(c->pm_tab.ensure(n * sizeof(double2)));
+    GG_TRY(cudaMemcpyAsync(c->pm_tab.p, tab.data(), n * sizeof(double2), cudaMemcpyHostToDevice, st));
+    GG_TRY(cudaStreamSynchronize(st));  // `tab` lives on this stack frame
+  }
   cufftSetStream((cufftHandle)c->pm_plan_f, st);
   cufftSetStream((cufftHandle)c->pm_plan_b, st);
   const double box = c->prm.box_size, d = box / n, f = n / box;
@@ -203,7 +221,7 @@ cudaError_t pm_stage(gpugrav_ctx *c, int pmgrid, int64_t np, const double *pos, 
   cufftResult r = cufftExecD2Z((cufftHandle)c->pm_plan_f, c->pm_rho.as<double>(), c->pm_rhok.as<cufftDoubleComplex>());
   if(r == CUFFT_SUCCESS)
     {
-      k_pm_green<<<blocks_for(NC), 256, 0, st>>>(n, 2.0 * M_PI / box, c->prm.asmth * c->prm.asmth, 0.5 * d,
+      k_pm_green<<<blocks_for(NC), 256, 0, st>>>(n, 2.0 * M_PI / box, c->pm_tab.as<double2>(),
                                                   c->pm_rhok.as<cufftDoubleComplex>());
       GG_TRY(cudaGetLastError());
       r = cufftExecZ2D((cufftHandle)c->pm_plan_b, c->pm_rhok.as<cufftDoubleComplex>(), c->pm_rho.as<double>());
@@ -229,5 +247,6 @@ void pm_release(gpugrav_ctx *c)
     }
   c->pm_rho.release();
   c->pm_rhok.release();
+  c->pm_tab.release();
 }
 }  // namespace gg

@@ -833,10 +833,23 @@ __global__ void k_depth_hist(const uint8_t *__restrict__ depth, int64_t nn, int 
       atomicAdd(&hist[t], h[t]);
 }
 
+// Nodes into depth buckets.  The order inside a bucket is free (every node of a level is
+// processed independently), so the lanes of a warp that share a depth take one atomic together.
 __global__ void k_depth_scatter(const uint8_t *__restrict__ depth, int64_t nn, int *cursor, int32_t *order)
 {
+  const int lane = threadIdx.x & 31;
   for(int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nn; k += (int64_t)gridDim.x * blockDim.x)
-    order[atomicAdd(&cursor[depth[k]], 1)] = (int32_t)k;
+    {
+      const unsigned act   = __activemask();
+      const int d          = depth[k];
+      const unsigned peers = __match_any_sync(act, d);
+      const int leader     = __ffs(peers) - 1;
+      int base             = 0;
+      if(lane == leader)
+        base = atomicAdd(&cursor[d], __popc(peers));
+      base = __shfl_sync(peers, base, leader);
+      order[base + __popc(peers & ((1u << lane) - 1u))] = (int32_t)k;
+    }
 }
 
 // ---- moments of one depth level (force_update_node_recursive, src/gravity/forcetree.c:1266-1392) ----
