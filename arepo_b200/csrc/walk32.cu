@@ -42,7 +42,7 @@ constexpr int kWarps   = GG_W32_WARPS;    // warps per block
 constexpr int kEvalAt  = GG_W32_EVAL_AT;  // evaluate once this many entries are queued
 constexpr int kUnroll  = GG_W32_UNROLL;   // list entries in flight per lane in the evaluation loop
 #ifndef GG_W32_MINBLOCKS
-#define GG_W32_MINBLOCKS 6
+#define GG_W32_MINBLOCKS 5  // blocks per SM the register budget is sized for (96 registers a thread)
 #endif
 // capacity: accepted nodes (<= 32) join a list holding fewer than kEvalAt entries; particles are
 // added at most 32 per round and the list is evaluated first whenever a round could overflow it
@@ -81,8 +81,7 @@ struct W32Const
   float theta2, erracc;
   int periodic, bh;
   float soft[GPUGRAV_MAX_SOFTTYPES + 1];
-  float2 tab[kNtab + 1];   // (f[i], f[i+1] - f[i]) of the force table
-  float2 tabp[kNtab + 1];  // same for the potential table
+  float4 tab[kNtab + 1];  // (f[i], f[i+1] - f[i], p[i], p[i+1] - p[i]) of the force and potential tables
   const float4 *ewd;       // Ewald correction (fx, fy, fz, pot) per table entry (pure periodic tree)
   float ewd_fac;           // 2 EN / L
   int mns;                 // MULTIPLE_NODE_SOFTENING: nodes used per softening type
@@ -192,6 +191,12 @@ __device__ __forceinline__ float wminf(float v)
     v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
+__device__ __forceinline__ float wmaxf(float v)
+{
+  for(int o = 16; o > 0; o >>= 1)
+    v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
 __device__ __forceinline__ int wscan_incl(int v, int lane)
 {
   for(int o = 1; o < 32; o <<= 1)
@@ -212,15 +217,18 @@ __device__ __forceinline__ float rsqrt_normal(float x)
   return y;
 }
 
-// Table index without conversion instructions: adding 1.5 * 2^23 leaves round(te - 0.5)
-// (= floor(te) up to ties, where both neighbours give the same interpolated value) in the
-// low mantissa bits.
-__device__ __forceinline__ float2 tab_lookup(const float2 *tab, float te, float &tw)
+// Short-range factors of the TreePM split at separation r: linear interpolation of the force and
+// potential tables between nodes floor(te) and floor(te) + 1, te = r * asmthfac, as the reference
+// does (src/gravity/forcetree_walk.c:366-379).  Adding 1.5 * 2^23 with rounding toward minus
+// infinity leaves floor(te) in the low mantissa bits (no conversion instruction); the index is
+// clamped to the last interval, which only entries beyond Rcut reach (they are masked).
+__device__ __forceinline__ void short_range(float r, const W32Const &w, float &ff, float &fpt)
 {
-  const float tb0 = (te - 0.5f) + 12582912.0f;
-  const int ti    = __float_as_int(tb0) - 0x4B400000;
-  tw              = te - (tb0 - 12582912.0f);
-  return tab[ti];
+  const float tb0 = fminf(__fmaf_rd(r, w.asmthfac, 12582912.0f), 12582912.0f + (float)(kNtab - 1));
+  const float tw  = fmaf(r, w.asmthfac, 12582912.0f - tb0);
+  const float4 t  = w.tab[__float_as_int(tb0) - 0x4B400000];
+  ff              = fmaf(tw, t.y, t.x);
+  fpt             = fmaf(tw, t.w, t.z);
 }
 
 // Per-target state of a lane (targets per lane: TPL).
@@ -257,86 +265,65 @@ __device__ __forceinline__ float4 ewald_corr32(float dx, float dy, float dz, con
   return make_float4(sx * r.x, sy * r.y, sz * r.z, r.w);
 }
 
-// One target against one list entry.  An entry beyond Rcut of this target (periodic) is
-// masked, not branched around; the softening branch is taken only inside the spline support.
-// EWALD: pure periodic tree (nearest image, no split), plus the Ewald correction of the entry.
-template <bool PERIODIC, bool POT, bool EWALD = false>
-__device__ __forceinline__ void interact(const float4 e, const float hj, Tgt &T, const W32Const &w)
+// Separation of a list entry from a target: (dx, dy, dz) = entry - target, r^2, 1/r and r.  A zero
+// separation (the target itself) gives a huge 1/r but r = 0; it always lies inside the softening
+// length.  far() and near() both call this, so they agree on which side of the softening length
+// every pair lies.
+struct Sep
 {
-  const float dx   = e.x - T.x, dy = e.y - T.y, dz = e.z - T.z;
-  const float r2   = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  const float hmax = fmaxf(T.h, hj);
-  // a zero separation (the target itself) gives a huge rinv but r = 0: the spline branch,
-  // whose periodic term is skipped at r = 0, handles it
-  const float rinv = rsqrt_normal(fmaxf(r2, 1.0e-30f));
-  const float r    = r2 * rinv;
-  bool in          = true;
+  float dx, dy, dz, r2, rinv, r;
+};
+__device__ __forceinline__ Sep separation(const float4 e, const Tgt &T)
+{
+  Sep s;
+  s.dx   = e.x - T.x;
+  s.dy   = e.y - T.y;
+  s.dz   = e.z - T.z;
+  s.r2   = fmaf(s.dx, s.dx, fmaf(s.dy, s.dy, s.dz * s.dz));
+  s.rinv = rsqrt_normal(fmaxf(s.r2, 1.0e-30f));
+  s.r    = s.r2 * s.rinv;
+  return s;
+}
+
+// One target against one list entry, outside the softening length (r >= max(h_i, h_j)): the
+// Newtonian kernel, times the TreePM short-range factor when PERIODIC.  An entry beyond Rcut of this
+// target (periodic) is masked, not branched around, so that the interactions of an unrolled block
+// schedule together.  CHECK: the entry may lie inside the softening length of this target; such a
+// pair is masked as well and reported by the return value, and near() adds the spline kernel for
+// it.  Without CHECK the list entry is known to lie outside the softening length of every target
+// of the group.  The interaction count and the Ewald correction (EWALD: pure periodic tree, nearest
+// image) are taken here for every pair.
+template <bool PERIODIC, bool POT, bool EWALD = false, bool CHECK = true>
+__device__ __forceinline__ bool far(const float4 e, const float hj, Tgt &T, const W32Const &w)
+{
+  const Sep s = separation(e, T);
+  bool in     = true;
   float ff = 0.0f, fpt = 0.0f;
   if(PERIODIC)
     {
-      in = r2 < w.rcut2;
-      // inside Rcut te < NTAB; the clamp (just below NTAB, so the last interval keeps its
-      // interpolation) only bounds the index of masked entries beyond Rcut
-      const float te = fminf(r * w.asmthfac, (float)kNtab - 0.0001f);
-      float tw;
-      const float2 tb = tab_lookup(w.tab, te, tw);
-      ff              = fmaf(tw, tb.y, tb.x);
+      in = s.r2 < w.rcut2;
+      short_range(s.r, w, ff, fpt);
+    }
+  float fac = s.rinv * s.rinv * s.rinv, wp = 0.0f;
+  if(PERIODIC)
+    {
+      fac = fmaf(s.rinv * ff, w.asmthinv2, fac);
       if(POT)
-        {
-          float tw2;
-          const float2 tp = tab_lookup(w.tabp, te, tw2);
-          fpt             = fmaf(tw2, tp.y, tp.x);
-        }
+        wp = s.rinv * fpt;
     }
-  float fac, wp = 0.0f;
-  if(r >= hmax)
-    {
-      fac = rinv * rinv * rinv;
-      if(PERIODIC)
-        {
-          fac = fmaf(rinv * ff, w.asmthinv2, fac);
-          if(POT)
-            wp = rinv * fpt;
-        }
-      else if(POT)
-        wp = -rinv;
-    }
-  else
-    {
-      const float h_inv  = 1.0f / hmax;
-      const float h3_inv = h_inv * h_inv * h_inv;
-      const float u      = r * h_inv;
-      const float u2     = u * u;
-      if(u < 0.5f)
-        {
-          fac = h3_inv * fmaf(u2, fmaf(SF2, u, SF3), SF1);
-          if(POT)
-            wp = h_inv * fmaf(u2, fmaf(u2, fmaf(SF6, u, SF7), SF5), SF4);
-        }
-      else
-        {
-          const float u3 = u2 * u;
-          fac = h3_inv * (SF8 + SF9 * u + SF10 * u2 + SF11 * u3 + SF12 / u3);
-          if(POT)
-            wp = h_inv * (SF13 + SF14 / u + u2 * (SF1 + u * (SF15 + u * (SF16 + SF17 * u))));
-        }
-      if(PERIODIC && r > 0.0f)
-        {
-          fac = fmaf(rinv * ff, w.asmthinv2, fac);
-          if(POT)
-            wp = fmaf(rinv, fpt + 1.0f, wp);
-        }
-    }
-  const float m  = in ? e.w : 0.0f;
-  const float fm = fac * m;
-  T.ax           = fmaf(dx, fm, T.ax);
-  T.ay           = fmaf(dy, fm, T.ay);
-  T.az           = fmaf(dz, fm, T.az);
+  else if(POT)
+    wp = -s.rinv;
+  const bool soft = CHECK && s.r < fmaxf(T.h, hj);
+  const float m   = in ? e.w : 0.0f;
+  const float fm  = soft ? 0.0f : fac * m;  // fac overflows at r = 0: select, do not multiply by 0
+  T.ax            = fmaf(s.dx, fm, T.ax);
+  T.ay            = fmaf(s.dy, fm, T.ay);
+  T.az            = fmaf(s.dz, fm, T.az);
   if(POT)
-    T.pot = fmaf(m, wp, T.pot);
+    T.pot = fmaf(soft ? 0.0f : m, wp, T.pot);
   if(EWALD)
     {
-      const float4 c = ewald_corr32(dx, dy, dz, w);
+      const float4 c = ewald_corr32(s.dx, s.dy, s.dz, w);
       T.ax           = fmaf(m, c.x, T.ax);
       T.ay           = fmaf(m, c.y, T.ay);
       T.az           = fmaf(m, c.z, T.az);
@@ -344,10 +331,59 @@ __device__ __forceinline__ void interact(const float4 e, const float hj, Tgt &T,
         T.pot = fmaf(m, c.w, T.pot);
     }
   T.ni += in ? 1 : 0;  // list entries all have mass != 0
+  return soft;
 }
 
-// The lane's TPL targets against `nl` list entries (each entry read once for all of them),
-// then the batch partials are folded into the FP64 sums.
+// The softened kernel of one target against one list entry, for a pair inside the softening length
+// (nothing otherwise): the reference's spline (src/gravity/forcetree_walk.c:421-455), plus the
+// TreePM short-range correction of the Newtonian part away from r = 0.
+template <bool PERIODIC, bool POT>
+__device__ __forceinline__ void near(const float4 e, const float hj, Tgt &T, const W32Const &w)
+{
+  const Sep s      = separation(e, T);
+  const float hmax = fmaxf(T.h, hj);
+  if(!(s.r < hmax))
+    return;
+  const float h_inv  = 1.0f / hmax;
+  const float h3_inv = h_inv * h_inv * h_inv;
+  const float u      = s.r * h_inv;
+  const float u2     = u * u;
+  float fac, wp = 0.0f;
+  if(u < 0.5f)
+    {
+      fac = h3_inv * fmaf(u2, fmaf(SF2, u, SF3), SF1);
+      if(POT)
+        wp = h_inv * fmaf(u2, fmaf(u2, fmaf(SF6, u, SF7), SF5), SF4);
+    }
+  else
+    {
+      const float u3 = u2 * u;
+      fac = h3_inv * (SF8 + SF9 * u + SF10 * u2 + SF11 * u3 + SF12 / u3);
+      if(POT)
+        wp = h_inv * (SF13 + SF14 / u + u2 * (SF1 + u * (SF15 + u * (SF16 + SF17 * u))));
+    }
+  bool in = true;
+  if(PERIODIC)
+    {
+      in = s.r2 < w.rcut2;
+      if(s.r > 0.0f)
+        {
+          float ff, fpt;
+          short_range(s.r, w, ff, fpt);
+          fac = fmaf(s.rinv * ff, w.asmthinv2, fac);
+          if(POT)
+            wp = fmaf(s.rinv, fpt + 1.0f, wp);
+        }
+    }
+  const float m  = in ? e.w : 0.0f;
+  const float fm = fac * m;
+  T.ax           = fmaf(s.dx, fm, T.ax);
+  T.ay           = fmaf(s.dy, fm, T.ay);
+  T.az           = fmaf(s.dz, fm, T.az);
+  if(POT)
+    T.pot = fmaf(m, wp, T.pot);
+}
+
 #ifdef GG_WALK32_STATS
 }  // namespace
 // measurement build only: [0] list entries evaluated per lane, [1] node tests, [2] particle candidates,
@@ -370,19 +406,63 @@ namespace
   while(0)
 #endif
 
-template <bool PERIODIC, bool POT, int TPL, bool EWALD = false>
-__device__ __forceinline__ void evaluate(const float4 *__restrict__ LP, const float *__restrict__ LH, int nl, Tgt (&T)[TPL],
-                                         const W32Const &w)
+// The lane's TPL targets against the warp's list (each entry read once for all of them), in blocks
+// of kUnroll entries evaluated without branches.  The list has two regions: `nf` far entries at the
+// bottom of the buffer, outside the softening length of every target of the group, and `nn` near
+// entries at the top, for which a block in which some pair lies inside the softening length (the
+// targets' own particles, close neighbours) is revisited for those pairs.  Then the batch partials
+// are folded into the FP64 sums.
+template <bool PERIODIC, bool POT, int TPL, bool EWALD, bool CHECK>
+__device__ __forceinline__ void evaluate_region(const float4 *__restrict__ LP, const float *__restrict__ LH, int nl, Tgt (&T)[TPL],
+                                                const W32Const &w)
 {
-#pragma unroll kUnroll
-  for(int j = 0; j < nl; j++)
+  int j = 0;
+  for(; j + kUnroll <= nl; j += kUnroll)
+    {
+      float4 e[kUnroll];
+      float hj[kUnroll];
+#pragma unroll
+      for(int u = 0; u < kUnroll; u++)
+        {
+          e[u]  = LP[j + u];
+          hj[u] = LH[j + u];
+        }
+      bool soft = false;
+#pragma unroll
+      for(int u = 0; u < kUnroll; u++)
+#pragma unroll
+        for(int k = 0; k < TPL; k++)
+          soft |= far<PERIODIC, POT, EWALD, CHECK>(e[u], hj[u], T[k], w);
+      if(CHECK && soft)
+        {
+#pragma unroll 1
+          for(int u = 0; u < kUnroll; u++)
+            {
+              const float4 eu = LP[j + u];
+              const float hu  = LH[j + u];
+#pragma unroll
+              for(int k = 0; k < TPL; k++)
+                near<PERIODIC, POT>(eu, hu, T[k], w);
+            }
+        }
+    }
+  for(; j < nl; j++)
     {
       const float4 e = LP[j];
       const float hj = LH[j];
 #pragma unroll
       for(int k = 0; k < TPL; k++)
-        interact<PERIODIC, POT, EWALD>(e, hj, T[k], w);
+        if(far<PERIODIC, POT, EWALD, CHECK>(e, hj, T[k], w) && CHECK)
+          near<PERIODIC, POT>(e, hj, T[k], w);
     }
+}
+
+template <bool PERIODIC, bool POT, int TPL, bool EWALD = false>
+__device__ __forceinline__ void evaluate(const float4 *__restrict__ LP, const float *__restrict__ LH, int nf, int nn, Tgt (&T)[TPL],
+                                         const W32Const &w)
+{
+  evaluate_region<PERIODIC, POT, TPL, EWALD, false>(LP, LH, nf, T, w);
+  evaluate_region<PERIODIC, POT, TPL, EWALD, true>(LP + kListCap - nn, LH + kListCap - nn, nn, T, w);
 #pragma unroll
   for(int k = 0; k < TPL; k++)
     {
@@ -392,6 +472,22 @@ __device__ __forceinline__ void evaluate(const float4 *__restrict__ LP, const fl
       T[k].dpot += T[k].pot;
       T[k].ax = T[k].ay = T[k].az = T[k].pot = 0.0f;
     }
+}
+
+// Appends one entry per lane that keeps one to the warp's list: to the far region (bottom, growing
+// up) or, `nr`, to the near region (top, growing down).
+__device__ __forceinline__ void push(float4 *LP, float *LH, int &nf, int &nn, bool keep, bool nr, const float4 e, float h,
+                                     unsigned lt_mask)
+{
+  const unsigned kf = __ballot_sync(0xffffffffu, keep && !nr), kn = __ballot_sync(0xffffffffu, keep && nr);
+  if(keep)
+    {
+      const int pos = nr ? kListCap - 1 - (nn + __popc(kn & lt_mask)) : nf + __popc(kf & lt_mask);
+      LP[pos]       = e;
+      LH[pos]       = h;
+    }
+  nf += __popc(kf);
+  nn += __popc(kn);
 }
 
 template <bool PERIODIC, bool POT, int TPL, bool EWALD = false>
@@ -443,7 +539,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
       WALK_STAT(3, 1);
       double4 p[TPL];
       double mnx = 1e300, mxx = -1e300, mny = 1e300, mxy = -1e300, mnz = 1e300, mxz = -1e300;
-      float hmin_l = 3.0e38f, amin_l = 3.0e38f, a_l[TPL];
+      float hmin_l = 3.0e38f, hmax_l = 0.0f, amin_l = 3.0e38f, a_l[TPL];
 #pragma unroll
       for(int k = 0; k < TPL; k++)
         {
@@ -455,6 +551,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
           mny = fmin(mny, p[k].y), mxy = fmax(mxy, p[k].y);
           mnz = fmin(mnz, p[k].z), mxz = fmax(mxz, p[k].z);
           hmin_l = fminf(hmin_l, w.soft[tst[tt]]);
+          hmax_l = fmaxf(hmax_l, w.soft[tst[tt]]);
           amin_l = fminf(amin_l, a_l[k]);
         }
       // group box (FP64), centre g, half extent (rounded up)
@@ -463,6 +560,9 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
       const float ex = (float)(0.5 * (mxx - mnx)) * 1.000001f, ey = (float)(0.5 * (mxy - mny)) * 1.000001f,
                   ez = (float)(0.5 * (mxz - mnz)) * 1.000001f;
       const float h_min    = wminf(hmin_l);
+      // an entry farther than max(h_grp, h_j) from the group box is outside the softening length of
+      // every target (the margin covers the rounding of the FP32 separations)
+      const float h_grp    = wmaxf(hmax_l) * 1.001f;
       const float aold_min = wminf(amin_l);
       // box side squared over kVote^2: a node smaller than this and closer than it gets the per-target vote
       const float side     = 2.0f * fmaxf(ex, fmaxf(ey, ez));
@@ -478,7 +578,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
           T[k].ni = 0;
         }
 
-      int nl = 0, sp = 1;
+      int nf = 0, nn = 0, sp = 1;  // list: far and near entries
       if(lane == 0)
         stack[0] = root;
       __syncwarp();
@@ -497,6 +597,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
           float4 entry = make_float4(0, 0, 0, 0);
           float hj     = 0;
           int fc = 0, fp = 0, nc = 0, np = 0;
+          float ent_d2 = 0.0f;  // squared distance of the entry from the group box
           bool vote = false, vote_keep = false;  // per-target vote pending; entry kept if accepted
           bool split = false;                    // MULTIPLE_NODE_SOFTENING: accepted node listed per type
           float4 vrel = make_float4(0, 0, 0, 0);   // centre - CoM, side of a voting node
@@ -552,6 +653,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                               vote_keep = !PERIODIC || rmin2 < w.rcut2;
                               vrel      = rel;
                               entry     = make_float4(sx, sy, sz, m);
+                              ent_d2    = rmin2;
                             }
                         }
                       else if(!PERIODIC || rmin2 < w.rcut2)
@@ -559,6 +661,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                           // accepted; a node whose CoM is beyond Rcut of every target contributes nothing
                           action = 1;
                           entry  = make_float4(sx, sy, sz, m);
+                          ent_d2 = rmin2;
                         }
                     }
                 }
@@ -599,35 +702,26 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                 }
             }
           // accepted nodes -> list (nodes used per softening type follow below)
-          const unsigned am = __ballot_sync(0xffffffffu, action == 1 && !split);
-          if(action == 1 && !split)
-            {
-              const int pos = nl + __popc(am & lt_mask);
-              LP[pos]       = entry;
-              LH[pos]       = hj;
-            }
-          nl += __popc(am);
+          {
+            const float hn = fmaxf(h_grp, hj);
+            push(LP, LH, nf, nn, action == 1 && !split, ent_d2 < hn * hn, entry, hj, lt_mask);
+          }
           // MULTIPLE_NODE_SOFTENING: one entry per softening type with that type's mass and softening
           // (forcetree_walk.c:382-401); for a target whose own softening exceeds the node's largest
           // this equals the single entry, the kernel being linear in the mass
           if(__ballot_sync(0xffffffffu, action == 1 && split))
             for(int t = 0; t < w.nsoft; t++)
               {
-                if(nl + 32 > kListCap)
+                if(nf + nn + 32 > kListCap)
                   {
-                    evaluate<PERIODIC, POT, TPL, EWALD>(LP, LH, nl, T, w);
-                    nl = 0;
+                    evaluate<PERIODIC, POT, TPL, EWALD>(LP, LH, nf, nn, T, w);
+                    nf = nn = 0;
                     __syncwarp();
                   }
-                const float mt    = (action == 1 && split) ? w.mpt[(int64_t)node * w.nsoft + t] : 0.0f;
-                const unsigned km = __ballot_sync(0xffffffffu, mt != 0.0f);
-                if(mt != 0.0f)
-                  {
-                    const int pos = nl + __popc(km & lt_mask);
-                    LP[pos]       = make_float4(entry.x, entry.y, entry.z, mt);
-                    LH[pos]       = w.soft[t];
-                  }
-                nl += __popc(km);
+                const float mt = (action == 1 && split) ? w.mpt[(int64_t)node * w.nsoft + t] : 0.0f;
+                const float hn = fmaxf(h_grp, w.soft[t]);
+                push(LP, LH, nf, nn, mt != 0.0f, ent_d2 < hn * hn, make_float4(entry.x, entry.y, entry.z, mt), w.soft[t],
+                     lt_mask);
               }
           // particles of opened nodes -> list, one particle per lane per round; particles beyond
           // Rcut of the whole group are dropped
@@ -638,10 +732,10 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
           WALK_STAT(2, ptot);
           for(int q0 = 0; q0 < ptot; q0 += 32)
             {
-              if(nl + 32 > kListCap)
+              if(nf + nn + 32 > kListCap)
                 {
-                  evaluate<PERIODIC, POT, TPL, EWALD>(LP, LH, nl, T, w);
-                  nl = 0;
+                  evaluate<PERIODIC, POT, TPL, EWALD>(LP, LH, nf, nn, T, w);
+                  nf = nn = 0;
                   __syncwarp();
                 }
               const int q = q0 + lane;
@@ -658,7 +752,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
               const int oexc = __shfl_sync(0xffffffffu, pexc, L);
               bool keep      = false;
               float4 pe      = make_float4(0, 0, 0, 0);
-              float ph       = 0;
+              float ph = 0, pd2 = 0;
               if(q < ptot)
                 {
                   const int pi     = ofp + (q - oexc);
@@ -667,21 +761,14 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                                    (float)pp.w);
                   ph   = w.soft[g_pst[pi]];
                   keep = pp.w != 0.0;
+                  const float dmx = fmaxf(fabsf(pe.x) - ex, 0.0f), dmy = fmaxf(fabsf(pe.y) - ey, 0.0f),
+                              dmz = fmaxf(fabsf(pe.z) - ez, 0.0f);
+                  pd2 = dmx * dmx + dmy * dmy + dmz * dmz;
                   if(PERIODIC)
-                    {
-                      const float dmx = fmaxf(fabsf(pe.x) - ex, 0.0f), dmy = fmaxf(fabsf(pe.y) - ey, 0.0f),
-                                  dmz = fmaxf(fabsf(pe.z) - ez, 0.0f);
-                      keep = keep && (dmx * dmx + dmy * dmy + dmz * dmz < w.rcut2);
-                    }
+                    keep = keep && pd2 < w.rcut2;
                 }
-              const unsigned km = __ballot_sync(0xffffffffu, keep);
-              if(keep)
-                {
-                  const int pos = nl + __popc(km & lt_mask);
-                  LP[pos]       = pe;
-                  LH[pos]       = ph;
-                }
-              nl += __popc(km);
+              const float hn = fmaxf(h_grp, ph);
+              push(LP, LH, nf, nn, keep, pd2 < hn * hn, pe, ph, lt_mask);
             }
           // node children of opened nodes -> stack (contiguous in breadth-first order)
           const int ncx  = (action == 2) ? nc : 0;
@@ -697,18 +784,18 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
           else if(lane == 0)
             atomicOr(err, 16);  // stack too small: the walk of this group is incomplete
           __syncwarp();
-          if(nl >= kEvalAt)
+          if(nf + nn >= kEvalAt)
             {
-              WALK_STAT(0, nl);
-              evaluate<PERIODIC, POT, TPL, EWALD>(LP, LH, nl, T, w);
-              nl = 0;
+              WALK_STAT(0, nf + nn);
+              evaluate<PERIODIC, POT, TPL, EWALD>(LP, LH, nf, nn, T, w);
+              nf = nn = 0;
               __syncwarp();
             }
         }
-      if(nl > 0)
+      if(nf + nn > 0)
         {
-          WALK_STAT(0, nl);
-          evaluate<PERIODIC, POT, TPL, EWALD>(LP, LH, nl, T, w);
+          WALK_STAT(0, nf + nn);
+          evaluate<PERIODIC, POT, TPL, EWALD>(LP, LH, nf, nn, T, w);
           __syncwarp();
         }
 #pragma unroll
@@ -884,8 +971,7 @@ void make_w32(const WalkConst &wc, W32Const *w)
     {
       float f0 = wc.tab_force[i], f1 = (i < kNtab) ? wc.tab_force[i + 1] : wc.tab_force[i];
       float p0 = wc.tab_pot[i], p1 = (i < kNtab) ? wc.tab_pot[i + 1] : wc.tab_pot[i];
-      w->tab[i]  = make_float2(f0, f1 - f0);
-      w->tabp[i] = make_float2(p0, p1 - p0);
+      w->tab[i] = make_float4(f0, f1 - f0, p0, p1 - p0);
     }
 }
 }  // namespace
