@@ -77,11 +77,11 @@ constexpr float kVote = 16.0f;
 struct W32Const
 {
   double box, half_box;
-  float rcut, rcut2, asmthfac, asmthinv2;
+  float rcut, rcut2, asmthfac, pad1;
   float theta2, erracc;
   int periodic, bh;
   float soft[GPUGRAV_MAX_SOFTTYPES + 1];
-  float4 tab[kNtab + 1];  // (f[i], f[i+1] - f[i], p[i], p[i+1] - p[i]) of the force and potential tables
+  float4 tab[kNtab + 1];  // (f[i], f[i+1] - f[i], p[i], p[i+1] - p[i]): force table times 1/Asmth^2, potential table
   const float4 *ewd;       // Ewald correction (fx, fy, fz, pot) per table entry (pure periodic tree)
   float ewd_fac;           // 2 EN / L
   int mns;                 // MULTIPLE_NODE_SOFTENING: nodes used per softening type
@@ -217,9 +217,9 @@ __device__ __forceinline__ float rsqrt_normal(float x)
   return y;
 }
 
-// Short-range factors of the TreePM split at separation r: linear interpolation of the force and
-// potential tables between nodes floor(te) and floor(te) + 1, te = r * asmthfac, as the reference
-// does (src/gravity/forcetree_walk.c:366-379).  Adding 1.5 * 2^23 with rounding toward minus
+// Short-range factors of the TreePM split at separation r: linear interpolation of the force
+// (scaled by 1/Asmth^2) and potential tables between nodes floor(te) and floor(te) + 1,
+// te = r * asmthfac, as the reference does (src/gravity/forcetree_walk.c:366-379).  Adding 1.5 * 2^23 with rounding toward minus
 // infinity leaves floor(te) in the low mantissa bits (no conversion instruction); the index is
 // clamped to the last interval, which only entries beyond Rcut reach (they are masked).
 __device__ __forceinline__ void short_range(float r, const W32Const &w, float &ff, float &fpt)
@@ -304,23 +304,17 @@ __device__ __forceinline__ bool far(const float4 e, const float hj, Tgt &T, cons
       in = s.r2 < w.rcut2;
       short_range(s.r, w, ff, fpt);
     }
-  float fac = s.rinv * s.rinv * s.rinv, wp = 0.0f;
-  if(PERIODIC)
-    {
-      fac = fmaf(s.rinv * ff, w.asmthinv2, fac);
-      if(POT)
-        wp = s.rinv * fpt;
-    }
-  else if(POT)
-    wp = -s.rinv;
+  // force m (1/r^3 + f_s / (r Asmth^2)) = (m/r) (1/r^2 + f_s'), potential (m/r) p_s (Newtonian: -m/r);
+  // 1/r^2 stays finite at the clamped r = 0, so masking m/r masks both
   const bool soft = CHECK && s.r < fmaxf(T.h, hj);
   const float m   = in ? e.w : 0.0f;
-  const float fm  = soft ? 0.0f : fac * m;  // fac overflows at r = 0: select, do not multiply by 0
+  const float mr  = soft ? 0.0f : m * s.rinv;
+  const float fm  = mr * (PERIODIC ? s.rinv * s.rinv + ff : s.rinv * s.rinv);
   T.ax            = fmaf(s.dx, fm, T.ax);
   T.ay            = fmaf(s.dy, fm, T.ay);
   T.az            = fmaf(s.dz, fm, T.az);
   if(POT)
-    T.pot = fmaf(soft ? 0.0f : m, wp, T.pot);
+    T.pot = PERIODIC ? fmaf(mr, fpt, T.pot) : T.pot - mr;
   if(EWALD)
     {
       const float4 c = ewald_corr32(s.dx, s.dy, s.dz, w);
@@ -370,7 +364,7 @@ __device__ __forceinline__ void near(const float4 e, const float hj, Tgt &T, con
         {
           float ff, fpt;
           short_range(s.r, w, ff, fpt);
-          fac = fmaf(s.rinv * ff, w.asmthinv2, fac);
+          fac = fmaf(s.rinv, ff, fac);
           if(POT)
             wp = fmaf(s.rinv, fpt + 1.0f, wp);
         }
@@ -957,7 +951,7 @@ void make_w32(const WalkConst &wc, W32Const *w)
   w->rcut      = (float)wc.rcut;
   w->rcut2     = (float)wc.rcut2;
   w->asmthfac  = (float)wc.asmthfac;
-  w->asmthinv2 = (float)wc.asmthinv2;
+  const double finv = wc.pm ? wc.asmthinv2 : 1.0;
   w->theta2    = (float)(wc.theta * wc.theta);
   w->erracc    = (float)wc.erracc;
   w->periodic  = wc.periodic;
@@ -969,7 +963,7 @@ void make_w32(const WalkConst &wc, W32Const *w)
     w->soft[i] = (float)wc.soft[i];
   for(int i = 0; i <= kNtab; i++)
     {
-      float f0 = wc.tab_force[i], f1 = (i < kNtab) ? wc.tab_force[i + 1] : wc.tab_force[i];
+      float f0 = (float)(finv * wc.tab_force[i]), f1 = (float)(finv * ((i < kNtab) ? wc.tab_force[i + 1] : wc.tab_force[i]));
       float p0 = wc.tab_pot[i], p1 = (i < kNtab) ? wc.tab_pot[i + 1] : wc.tab_pot[i];
       w->tab[i] = make_float4(f0, f1 - f0, p0, p1 - p0);
     }
