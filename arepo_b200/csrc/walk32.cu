@@ -266,13 +266,14 @@ __device__ __forceinline__ float4 ewald_corr32(float dx, float dy, float dz, con
 }
 
 // Separation of a list entry from a target: (dx, dy, dz) = entry - target, r^2, 1/r and r.  A zero
-// separation (the target itself) gives a huge 1/r but r = 0; it always lies inside the softening
-// length.  far() and near() both call this, so they agree on which side of the softening length
-// every pair lies.
+// separation (the target itself) gives a huge 1/r but r = 0 (CLAMP); it lies inside the softening
+// length unless that is zero, where the reference's kernel has no finite value either.  far() and
+// near() both call this, so they agree on which side of the softening length every pair lies.
 struct Sep
 {
   float dx, dy, dz, r2, rinv, r;
 };
+template <bool CLAMP = true>
 __device__ __forceinline__ Sep separation(const float4 e, const Tgt &T)
 {
   Sep s;
@@ -280,7 +281,7 @@ __device__ __forceinline__ Sep separation(const float4 e, const Tgt &T)
   s.dy   = e.y - T.y;
   s.dz   = e.z - T.z;
   s.r2   = fmaf(s.dx, s.dx, fmaf(s.dy, s.dy, s.dz * s.dz));
-  s.rinv = rsqrt_normal(fmaxf(s.r2, 1.0e-30f));
+  s.rinv = rsqrt_normal(CLAMP ? fmaxf(s.r2, 1.0e-30f) : s.r2);
   s.r    = s.r2 * s.rinv;
   return s;
 }
@@ -296,7 +297,8 @@ __device__ __forceinline__ Sep separation(const float4 e, const Tgt &T)
 template <bool PERIODIC, bool POT, bool EWALD = false, bool CHECK = true>
 __device__ __forceinline__ bool far(const float4 e, const float hj, Tgt &T, const W32Const &w)
 {
-  const Sep s = separation(e, T);
+  // outside every target's softening length (no CHECK) r > 0 unless the softening is zero
+  const Sep s = separation<CHECK>(e, T);
   bool in     = true;
   float ff = 0.0f, fpt = 0.0f;
   if(PERIODIC)
@@ -309,7 +311,7 @@ __device__ __forceinline__ bool far(const float4 e, const float hj, Tgt &T, cons
   const bool soft = CHECK && s.r < fmaxf(T.h, hj);
   const float m   = in ? e.w : 0.0f;
   const float mr  = soft ? 0.0f : m * s.rinv;
-  const float fm  = mr * (PERIODIC ? s.rinv * s.rinv + ff : s.rinv * s.rinv);
+  const float fm  = mr * (PERIODIC ? fmaf(s.rinv, s.rinv, ff) : s.rinv * s.rinv);
   T.ax            = fmaf(s.dx, fm, T.ax);
   T.ay            = fmaf(s.dy, fm, T.ay);
   T.az            = fmaf(s.dz, fm, T.az);
@@ -597,11 +599,12 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
           float4 vrel = make_float4(0, 0, 0, 0);   // centre - CoM, side of a voting node
           if(node >= 0)
             {
+              // the three records of the node are fetched together (one memory round trip)
               const double4 sm = g_sm[node];
+              const float4 rel = g_rel[node];
+              const int4 kd    = g_kids[node];
               if(sm.w != 0.0)
                 {
-                  const float4 rel = g_rel[node];
-                  const int4 kd    = g_kids[node];
                   const float sx = (float)wrapd(sm.x - gx, w), sy = (float)wrapd(sm.y - gy, w), sz = (float)wrapd(sm.z - gz, w);
                   const float cx = sx + rel.x, cy = sy + rel.y, cz = sz + rel.z;
                   const float L  = rel.w;
