@@ -45,7 +45,12 @@ __device__ __forceinline__ double nearest(double x, const WalkConst &w)
 
 constexpr int kWarps = 4;
 
-__global__ void __launch_bounds__(32 * kWarps) k_walk64(const double4 *__restrict__ w_sm, const double4 *__restrict__ w_cl,
+// EWALD (pure periodic tree) and MNS (MULTIPLE_NODE_SOFTENING) are compiled in only where used: the
+// TreePM and isolated walks keep the register budget of a kernel without them.  The walk is
+// latency-bound (lanes wait on the entry the warp serves): 6 blocks per SM (80 registers) measured
+// 1.1x faster than 5 (96 registers) on the zoom box.
+template <bool EWALD, bool MNS>
+__global__ void __launch_bounds__(32 * kWarps, 6) k_walk64(const double4 *__restrict__ w_sm, const double4 *__restrict__ w_cl,
                                                         const int2 *__restrict__ w_link, uint32_t n_entries,
                                                         const double4 *__restrict__ tpm, const uint8_t *__restrict__ tst,
                                                         const float *__restrict__ oldacc, int64_t t_begin, int64_t t_end,
@@ -165,7 +170,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk64(const double4 *__restric
           double h_j = w.soft[link.y & 0xff];
           if(h_j > h_i)
             {
-              if(w.mns)
+              if(MNS)
                 split = true;  // src/gravity/forcetree_walk.c:296-308
               else if(r2 < h_j * h_j)
                 {
@@ -195,7 +200,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk64(const double4 *__restric
               factor_pot       = (1.0 - tabweight) * w.tab_pot[tabindex] + tabweight * w.tab_pot[tabindex + 1];
             }
           // per softening type under MULTIPLE_NODE_SOFTENING (forcetree_walk.c:382-401), else once
-          const int t0 = split ? 0 : -1, t1 = split ? w.nsoft : 0;
+          const int t0 = (MNS && split) ? 0 : -1, t1 = (MNS && split) ? w.nsoft : 0;
           for(int type = t0; type < t1; type++)
             {
               if(type >= 0)
@@ -252,7 +257,7 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk64(const double4 *__restric
               acc_x += dx * fac;
               acc_y += dy * fac;
               acc_z += dz * fac;
-              if(w.ewald)
+              if(EWALD)
                 {
                   // all further periodic images, src/gravity/forcetree_walk.c:469-477
                   double fcorr[3], pcorr;
@@ -286,12 +291,13 @@ __global__ void __launch_bounds__(32 * kWarps) k_walk64(const double4 *__restric
 
 cudaError_t walk64_stage(gpugrav_ctx *c, const WalkConst &wc)
 {
-  (void)wc;
   const int64_t n       = c->n;
   const int64_t t_begin = n * c->slice / c->nslices, t_end = n * (c->slice + 1) / c->nslices;
   const int64_t warps   = (t_end - t_begin + 31) / 32;
   const int64_t blocks  = warps > 0 ? (warps + kWarps - 1) / kWarps : 1;
-  k_walk64<<<(unsigned)blocks, 32 * kWarps, 0, c->stream>>>(
+  auto kern = wc.ewald ? (wc.mns ? k_walk64<true, true> : k_walk64<true, false>)
+                       : (wc.mns ? k_walk64<false, true> : k_walk64<false, false>);
+  kern<<<(unsigned)blocks, 32 * kWarps, 0, c->stream>>>(
       c->w_sm.as<double4>(), c->w_cl.as<double4>(), c->w_link.as<int2>(), (uint32_t)c->n_entries, c->s_pm.as<double4>(),
       c->s_st.as<uint8_t>(), c->oldacc_s.as<float>(), t_begin, t_end, c->wconst.as<WalkConst>(), c->acc_s.as<double>(), c->pot_s.as<double>(),
       c->nint_s.as<int32_t>(), (unsigned long long *)(c->counters.as<int>() + 32));
