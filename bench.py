@@ -59,9 +59,10 @@ METRIC = "tree-gravity particles/s at N=2^24 (RMS force err ≤1e-3); serving p5
 UNIT = "particles/s"
 FLOPS_PER_INTERACTION = 23.0  # convention of the path's roofline
 # DRAM bytes (read + write) of one FP32 walk launch per particle: ncu capture of the zoom box at
-# N=2^21 (dram__bytes_read.sum + dram__bytes_write.sum = 299 MB + 90 MB), scaled by the particle
-# count (the walk reads the tree and the particles once from DRAM; everything else hits in L2)
-WALK32_DRAM_BYTES_PER_PARTICLE = 388.8e6 / (1 << 21)
+# N=2^21 (dram__bytes_read.sum + dram__bytes_write.sum = 284.5 MB + 78.4 MB), scaled by the
+# particle count (the walk reads the tree and the particles once from DRAM; everything else hits
+# in L2)
+WALK32_DRAM_BYTES_PER_PARTICLE = 362.9e6 / (1 << 21)
 
 
 def log(*a):
