@@ -47,10 +47,10 @@ constexpr int kWarps = 4;
 
 // EWALD (pure periodic tree) and MNS (MULTIPLE_NODE_SOFTENING) are compiled in only where used: the
 // TreePM and isolated walks keep the register budget of a kernel without them.  The walk is
-// latency-bound (lanes wait on the entry the warp serves): 6 blocks per SM (80 registers) measured
-// 1.1x faster than 5 (96 registers) on the zoom box.
+// latency-bound (lanes wait on the entry the warp serves), so occupancy beats spill-free code: on
+// the zoom box 12 blocks per SM (48 warps) walk 1.18x faster than 6 and 1.3x faster than 5.
 template <bool EWALD, bool MNS>
-__global__ void __launch_bounds__(32 * kWarps, 6) k_walk64(const double4 *__restrict__ w_sm, const double4 *__restrict__ w_cl,
+__global__ void __launch_bounds__(32 * kWarps, 12) k_walk64(const double4 *__restrict__ w_sm, const double4 *__restrict__ w_cl,
                                                         const int2 *__restrict__ w_link, uint32_t n_entries,
                                                         const double4 *__restrict__ tpm, const uint8_t *__restrict__ tst,
                                                         const float *__restrict__ oldacc, int64_t t_begin, int64_t t_end,
