@@ -9,12 +9,12 @@
 //      (sin(k d/2) / (k d/2))^-4 per axis, zero mode cleared (:1620-1704); both factors separate
 //      into per-axis tables;
 //   4. complex-to-real FFT: the potential mesh (unnormalised, as the FFTW backward transform);
-//   5. per particle, the 4-point finite difference of the potential,
+//   5. per component, the force mesh: the 4-point finite difference of the potential,
 //      fac ((4/3)(phi[-1] - phi[+1]) - (1/6)(phi[-2] - phi[+2])), fac = 4 pi G / L^3 / (2 d)
-//      (:1735-1790), at the 8 CIC nodes and the CIC-weighted sum (:1322-1538); the potential the
-//      same way with 4 pi G / L^3.  The reference first writes a force mesh per component; here
-//      the differences are formed at the particle from the potential mesh (L2-resident neighbours),
-//      which saves three mesh passes and gives the same sums.
+//      (:1735-1800), written into the complex buffer (free after the inverse transform), then
+//      read at the 8 CIC nodes of every particle and CIC-weighted (:1322-1538); the potential is
+//      read the same way from the potential mesh with 4 pi G / L^3.  One coalesced pass over the
+//      mesh per component keeps the particle reads at 8 per component instead of 13 per node.
 // G = 1 (accelerations without the factor G, like the tree walk).  The mesh is FP64 (the reference's
 // default fft_real is float; FP64 costs little here next to the tree walk).
 
@@ -101,8 +101,26 @@ __global__ void k_pm_green(int n, double kfac, const double2 *__restrict__ tab, 
     }
 }
 
-__global__ void k_pm_readout(int64_t np, const double *__restrict__ pos, int n, double f, double fac, double fac_pot,
-                             const double *__restrict__ phi, double *__restrict__ acc, double *__restrict__ pot, int *bad)
+// one component of the force mesh: the 4-point difference of the potential along `dim`
+__global__ void k_pm_fd(int n, int dim, double fac, const double *__restrict__ phi, double *__restrict__ force)
+{
+  const int64_t N = n, N3 = N * N * N;
+  const int64_t stride = dim == 0 ? N * N : (dim == 1 ? N : 1);
+  for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N3; i += (int64_t)gridDim.x * blockDim.x)
+    {
+      const int c = (int)((i / stride) % N);
+      auto at     = [&](int o) {
+        int q = c + o;
+        q     = q < 0 ? q + n : (q >= n ? q - n : q);
+        return phi[i + (int64_t)(q - c) * stride];
+      };
+      force[i] = fac * ((4.0 / 3) * (at(-1) - at(1)) - (1.0 / 6) * (at(-2) - at(2)));
+    }
+}
+
+// CIC readout of one mesh at every particle: out[ostride * i + ooff] = scale * sum_nodes w mesh
+__global__ void k_pm_cic_read(int64_t np, const double *__restrict__ pos, int n, double f, const double *__restrict__ mesh,
+                              double scale, double *__restrict__ out, int ostride, int ooff, int *bad)
 {
   const int64_t N = n;
   for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np; i += (int64_t)gridDim.x * blockDim.x)
@@ -116,33 +134,12 @@ __global__ void k_pm_readout(int64_t np, const double *__restrict__ pos, int n, 
           w[a][0] = 1.0 - d;
           w[a][1] = d;
         }
-      double ax = 0, ay = 0, az = 0, p = 0;
+      double v = 0;
       for(int ix = 0; ix < 2; ix++)
         for(int iy = 0; iy < 2; iy++)
           for(int iz = 0; iz < 2; iz++)
-            {
-              const int x = c[0][ix], y = c[1][iy], z = c[2][iz];
-              const double wt = w[0][ix] * w[1][iy] * w[2][iz];
-              auto at = [&](int xi, int yi, int zi) {
-                xi = xi < 0 ? xi + n : (xi >= n ? xi - n : xi);
-                yi = yi < 0 ? yi + n : (yi >= n ? yi - n : yi);
-                zi = zi < 0 ? zi + n : (zi >= n ? zi - n : zi);
-                return phi[(xi * N + yi) * N + zi];
-              };
-              const double fx = fac * ((4.0 / 3) * (at(x - 1, y, z) - at(x + 1, y, z)) - (1.0 / 6) * (at(x - 2, y, z) - at(x + 2, y, z)));
-              const double fy = fac * ((4.0 / 3) * (at(x, y - 1, z) - at(x, y + 1, z)) - (1.0 / 6) * (at(x, y - 2, z) - at(x, y + 2, z)));
-              const double fz = fac * ((4.0 / 3) * (at(x, y, z - 1) - at(x, y, z + 1)) - (1.0 / 6) * (at(x, y, z - 2) - at(x, y, z + 2)));
-              ax += fx * wt;
-              ay += fy * wt;
-              az += fz * wt;
-              if(pot)
-                p += phi[(x * N + y) * N + z] * wt;
-            }
-      acc[3 * i + 0] = ax;
-      acc[3 * i + 1] = ay;
-      acc[3 * i + 2] = az;
-      if(pot)
-        pot[i] = p * fac_pot;
+            v += mesh[(c[0][ix] * N + c[1][iy]) * N + c[2][iz]] * (w[0][ix] * w[1][iy] * w[2][iz]);
+      out[ostride * i + ooff] = v * scale;
     }
 }
 
@@ -232,8 +229,14 @@ cudaError_t pm_stage(gpugrav_ctx *c, int pmgrid, int64_t np, const double *pos, 
       return cudaSuccess;
     }
   const double fac_pot = 4.0 * M_PI / (box * box * box);
-  k_pm_readout<<<blocks_for(np), 256, 0, st>>>(np, pos, n, f, fac_pot / (2.0 * d), fac_pot, c->pm_rho.as<double>(), acc, pot,
-                                               bad);
+  double *force        = (double *)c->pm_rhok.p;  // n^2 (n/2+1) complex >= n^3 doubles
+  for(int dim = 0; dim < 3; dim++)
+    {
+      k_pm_fd<<<blocks_for(N3), 256, 0, st>>>(n, dim, fac_pot / (2.0 * d), c->pm_rho.as<double>(), force);
+      k_pm_cic_read<<<blocks_for(np), 256, 0, st>>>(np, pos, n, f, force, 1.0, acc, 3, dim, bad);
+    }
+  if(pot)
+    k_pm_cic_read<<<blocks_for(np), 256, 0, st>>>(np, pos, n, f, c->pm_rho.as<double>(), fac_pot, pot, 1, 0, bad);
   return cudaGetLastError();
 }
 
