@@ -21,6 +21,7 @@
 #include <map>
 #include <memory>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "internal.h"
@@ -428,7 +429,44 @@ cudaError_t serve_reserve(gpugrav_serve *s)
   return s->dl.ensure((size_t)n * 9 * sizeof(double));
 }
 
-// caller arrays -> pool at off, through the upload buffer: (x, y, z, m), (vx, vy, vz, 0), types
+// Host copy between the caller's (pageable) arrays and pinned staging.  One thread moves only a
+// few GB/s through pageable memory, so copies of several MB are split over up to 8 threads.
+void host_copy(void *dst, const void *src, size_t bytes)
+{
+  constexpr size_t kMinPerThread = 4u << 20;
+  unsigned t = std::thread::hardware_concurrency();
+  t          = t > 8 ? 8 : t;
+  if(bytes < 2 * kMinPerThread || t < 2)
+    {
+      memcpy(dst, src, bytes);
+      return;
+    }
+  if((size_t)t > bytes / kMinPerThread)
+    t = (unsigned)(bytes / kMinPerThread);
+  const size_t per = ((bytes + t - 1) / t + 4095) & ~(size_t)4095;
+  std::vector<std::thread> pool;
+  size_t done = per;  // the first piece is copied by this thread
+  try
+    {
+      for(; done < bytes; done += per)
+        {
+          const size_t len = bytes - done < per ? bytes - done : per;
+          pool.emplace_back([=] { memcpy((char *)dst + done, (const char *)src + done, len); });
+        }
+    }
+  catch(...)
+    {
+      // no thread to be had: copy the rest here
+      memcpy((char *)dst + done, (const char *)src + done, bytes - done);
+    }
+  memcpy(dst, src, per < bytes ? per : bytes);
+  for(auto &th : pool)
+    th.join();
+}
+
+// caller arrays -> pool at off, through the upload buffer: (x, y, z, m), (vx, vy, vz, 0), types.
+// When the pinned staging (reserved at creation) holds the request, the arrays are packed there and
+// sent in one DMA; the call then waits for it, since the staging serves the next copy too.
 cudaError_t upload(gpugrav_serve *s, int64_t off, int64_t n, const double *pos, const double *vel, const double *mass,
                    const uint8_t *st)
 {
@@ -436,10 +474,24 @@ cudaError_t upload(gpugrav_serve *s, int64_t off, int64_t n, const double *pos, 
   GG_TRY(s->up.ensure((size_t)n * (7 * sizeof(double) + 1)));
   double *din  = s->up.as<double>();
   uint8_t *dst = (uint8_t *)(din + 7 * n);
-  GG_TRY(cudaMemcpyAsync(din, pos, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice, q));
-  GG_TRY(cudaMemcpyAsync(din + 3 * n, vel, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice, q));
-  GG_TRY(cudaMemcpyAsync(din + 6 * n, mass, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, q));
-  GG_TRY(cudaMemcpyAsync(dst, st, n, cudaMemcpyHostToDevice, q));
+  const size_t bytes = (size_t)n * (7 * sizeof(double) + 1);
+  if(bytes <= s->staging.cap)
+    {
+      double *h = (double *)s->staging.p;
+      host_copy(h, pos, (size_t)n * 3 * sizeof(double));
+      host_copy(h + 3 * n, vel, (size_t)n * 3 * sizeof(double));
+      host_copy(h + 6 * n, mass, (size_t)n * sizeof(double));
+      memcpy(h + 7 * n, st, n);
+      GG_TRY(cudaMemcpyAsync(din, h, bytes, cudaMemcpyHostToDevice, q));
+      GG_TRY(cudaStreamSynchronize(q));
+    }
+  else
+    {
+      GG_TRY(cudaMemcpyAsync(din, pos, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice, q));
+      GG_TRY(cudaMemcpyAsync(din + 3 * n, vel, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice, q));
+      GG_TRY(cudaMemcpyAsync(din + 6 * n, mass, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, q));
+      GG_TRY(cudaMemcpyAsync(dst, st, n, cudaMemcpyHostToDevice, q));
+    }
   k_srv_unpack<<<grid_for(n, 256), 256, 0, q>>>(n, off, din, dst, s->pos.as<double4>(), s->vel.as<double4>(),
                                                 s->stype.as<uint8_t>());
   return cudaGetLastError();
@@ -609,9 +661,9 @@ int32_t gpugrav_serve_submit(gpugrav_serve *s, int64_t id, int64_t n, const doub
           delete r;
           return sfail(s, GPUGRAV_ERR_OOM, "request copy");
         }
-      memcpy(r->in.get(), pos, 3 * n * sizeof(double));
-      memcpy(r->in.get() + 3 * n, vel, 3 * n * sizeof(double));
-      memcpy(r->in.get() + 6 * n, mass, n * sizeof(double));
+      host_copy(r->in.get(), pos, 3 * n * sizeof(double));
+      host_copy(r->in.get() + 3 * n, vel, 3 * n * sizeof(double));
+      host_copy(r->in.get() + 6 * n, mass, n * sizeof(double));
       memcpy(r->st.get(), softtype, n);
     }
   r->t_submit = now_s();
@@ -927,11 +979,11 @@ int32_t gpugrav_serve_poll(gpugrav_serve *s, int64_t *id, int64_t *n, double *po
       SCK(cudaStreamSynchronize(st), "download");
       const char *h = (const char *)s->staging.p;
       if(pos)
-        memcpy(pos, h, b);
+        host_copy(pos, h, b);
       if(vel)
-        memcpy(vel, h + b, b);
+        host_copy(vel, h + b, b);
       if(acc)
-        memcpy(acc, h + 2 * b, b);
+        host_copy(acc, h + 2 * b, b);
     }
   pool_free(s, r->pool_off, r->n);
   if(times)

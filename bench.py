@@ -273,7 +273,7 @@ def run_stream(systems, ids, arrivals, max_systems, device, max_particles):
         nres = sum(len(systems[int(i)][2]) for i in ids)
         outbufs = None
         if nres * 72 <= 8e9:
-            outbufs = {int(i): tuple(np.zeros((len(systems[int(i)][2]), 3)) for _ in range(3)) for i in ids}
+            outbufs = {int(i): tuple(np.full((len(systems[int(i)][2]), 3), 0.0) for _ in range(3)) for i in ids}
         k, nsys_ticks = 0, 0
         t_sub = t_poll = 0.0
         t0 = time.monotonic()

@@ -262,8 +262,9 @@ int32_t gpugrav_direct(gpugrav_ctx *ctx, int64_t ntargets, const int64_t *target
  * drift_particle, src/time_integration/predict.c:357-425), with the FP32 walk.
  * Requests are admitted at tick boundaries in arrival order while system slots, the particle pool
  * and the device-memory budget allow; gpugrav_serve_tick advances every admitted system by one
- * force evaluation in one batched build and one persistent walk. Results stay on the host until
- * polled. No counterpart in the reference (it integrates one system per run). */
+ * force evaluation in one batched build and one persistent walk. Results stay in device memory
+ * until polled. A serving handle has no internal lock: call it from one host thread at a time.
+ * No counterpart in the reference (it integrates one system per run). */
 typedef struct gpugrav_serve gpugrav_serve;
 
 typedef struct gpugrav_serve_config
