@@ -153,12 +153,16 @@ CPU_SAMPLE_LOG2_HALF = 19   # N = 2^20 particles of the same zoom distribution
 CPU_SAMPLE_STRIDE = 64      # walk every 64th target, extrapolated to all
 
 
-def run_cpu_reference(procs: int, alpha: float, log2_half: int = CPU_SAMPLE_LOG2_HALF, stride: int = CPU_SAMPLE_STRIDE):
+def run_cpu_reference(procs: int, alpha: float, log2_half: int | None = None, stride: int | None = None):
     """Reference step on the host: domain decomposition (keys, sort, top tree), construct_forcetree,
     force_treeevaluate for a 1/stride sample of targets after a Barnes-Hut pass, by `procs` independent
-    processes that each walk a disjoint slice of the sample. Returns (particles/s, detail)."""
+    processes that each walk a disjoint slice of the sample. Returns (particles/s, detail).
+    The sample defaults to CPU_SAMPLE_LOG2_HALF / CPU_SAMPLE_STRIDE, read at call time."""
     from arepo_b200 import ics
     from oracle import oracle as O
+
+    log2_half = CPU_SAMPLE_LOG2_HALF if log2_half is None else log2_half
+    stride = CPU_SAMPLE_STRIDE if stride is None else stride
 
     exe = os.path.join(O.REF_DIR, "ref_harness_pm")
     if not os.path.exists(exe):
