@@ -101,20 +101,38 @@ __global__ void k_pm_green(int n, double kfac, const double2 *__restrict__ tab, 
     }
 }
 
-// one component of the force mesh: the 4-point difference of the potential along `dim`
+// one component of the force mesh: the 4-point difference of the potential along `dim`.  One block
+// per mesh row (x, y), threads along z: coordinates without a per-point division, coalesced rows.
 __global__ void k_pm_fd(int n, int dim, double fac, const double *__restrict__ phi, double *__restrict__ force)
 {
-  const int64_t N = n, N3 = N * N * N;
-  const int64_t stride = dim == 0 ? N * N : (dim == 1 ? N : 1);
-  for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N3; i += (int64_t)gridDim.x * blockDim.x)
+  const int64_t N = n;
+  auto wrap       = [n](int q) { return q < 0 ? q + n : (q >= n ? q - n : q); };
+  for(int64_t row = blockIdx.x; row < N * N; row += gridDim.x)
     {
-      const int c = (int)((i / stride) % N);
-      auto at     = [&](int o) {
-        int q = c + o;
-        q     = q < 0 ? q + n : (q >= n ? q - n : q);
-        return phi[i + (int64_t)(q - c) * stride];
-      };
-      force[i] = fac * ((4.0 / 3) * (at(-1) - at(1)) - (1.0 / 6) * (at(-2) - at(2)));
+      const int x = (int)(row / N), y = (int)(row % N);
+      const double *r0 = phi + row * N;
+      // the rows (dim 0: x +- 1, 2; dim 1: y +- 1, 2) or this row (dim 2) holding the four neighbours
+      const double *rm1 = r0, *rp1 = r0, *rm2 = r0, *rp2 = r0;
+      if(dim == 0)
+        {
+          rm1 = phi + (wrap(x - 1) * N + y) * N;
+          rp1 = phi + (wrap(x + 1) * N + y) * N;
+          rm2 = phi + (wrap(x - 2) * N + y) * N;
+          rp2 = phi + (wrap(x + 2) * N + y) * N;
+        }
+      else if(dim == 1)
+        {
+          rm1 = phi + (x * N + wrap(y - 1)) * N;
+          rp1 = phi + (x * N + wrap(y + 1)) * N;
+          rm2 = phi + (x * N + wrap(y - 2)) * N;
+          rp2 = phi + (x * N + wrap(y + 2)) * N;
+        }
+      for(int z = threadIdx.x; z < n; z += blockDim.x)
+        {
+          const int zm1 = dim == 2 ? wrap(z - 1) : z, zp1 = dim == 2 ? wrap(z + 1) : z;
+          const int zm2 = dim == 2 ? wrap(z - 2) : z, zp2 = dim == 2 ? wrap(z + 2) : z;
+          force[row * N + z] = fac * ((4.0 / 3) * (rm1[zm1] - rp1[zp1]) - (1.0 / 6) * (rm2[zm2] - rp2[zp2]));
+        }
     }
 }
 
@@ -232,7 +250,9 @@ cudaError_t pm_stage(gpugrav_ctx *c, int pmgrid, int64_t np, const double *pos, 
   double *force        = (double *)c->pm_rhok.p;  // n^2 (n/2+1) complex >= n^3 doubles
   for(int dim = 0; dim < 3; dim++)
     {
-      k_pm_fd<<<blocks_for(N3), 256, 0, st>>>(n, dim, fac_pot / (2.0 * d), c->pm_rho.as<double>(), force);
+      const int64_t rows = (int64_t)n * n;
+      k_pm_fd<<<(int)(rows < 148 * 16 ? rows : 148 * 16), 256, 0, st>>>(n, dim, fac_pot / (2.0 * d), c->pm_rho.as<double>(),
+                                                                          force);
       k_pm_cic_read<<<blocks_for(np), 256, 0, st>>>(np, pos, n, f, force, 1.0, acc, 3, dim, bad);
     }
   if(pot)
