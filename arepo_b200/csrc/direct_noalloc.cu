@@ -20,9 +20,16 @@
 //    it reads before reading it, so nothing has to start at zero and no state
 //    carries over, but two calls whose kernels overlap on the GPU (different
 //    streams, or host threads) race on the array: serialise them;
-//  * the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture.
+//  * the first call in a CUDA context looks up the array's device address in that
+//    context (cudaGetSymbolAddress, with the device current); make that first
+//    call before any stream capture.  The address is kept per context: a caller
+//    that drives the device through its own (non-primary) context gets that
+//    context's copy of the array;
+//  * softening types must lie in [0, nsofttypes): a target of another type gets
+//    NaN outputs, and a source of another type makes the outputs of every target
+//    it interacts with NaN (no softening length exists for it).
+#include <mutex>
+
 #include "internal.h"
 
 namespace
@@ -34,7 +41,37 @@ constexpr int kTile       = 128;
 // partial sums (acc.x, acc.y, acc.z, pot) per (source chunk, target)
 static __device__ __align__(256) double4 g_noalloc_partial[kChunks * kMaxTargets];
 
-double4 *g_partial_addr[64] = {nullptr};
+// device address of g_noalloc_partial per CUDA context (looked up once per context)
+struct ScratchAddr
+{
+  void *ctx;
+  double4 *addr;
+};
+constexpr int kMaxContexts = 64;
+ScratchAddr g_scratch_addr[kMaxContexts];
+int g_scratch_n = 0;
+std::mutex g_scratch_mu;
+
+// cuCtxGetCurrent through the runtime's driver entry point (no link dependency on libcuda)
+typedef int (*CtxGetCurrentFn)(void **);
+CtxGetCurrentFn ctx_get_current()
+{
+  static CtxGetCurrentFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if(cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+      fn = (CtxGetCurrentFn)f;
+  });
+  return fn;
+}
+
+// softening length of type t, NaN for a type without one (t >= nsofttypes)
+__device__ __forceinline__ double soft_of(const gg::WalkConst &w, unsigned t)
+{
+  return t < (unsigned)w.nsoft ? w.soft[t] : __longlong_as_double(0x7ff8000000000000ll);
+}
 
 #define SF1 10.666666666667
 #define SF2 32.0
@@ -72,7 +109,7 @@ __global__ void __launch_bounds__(kTile) k_direct_noalloc(const double *__restri
       mx  = tpos[3 * t + 0];
       my  = tpos[3 * t + 1];
       mz  = tpos[3 * t + 2];
-      h_i = w.soft[tst[t]];
+      h_i = soft_of(w, tst[t]);
     }
   const double asmth = w.periodic ? (0.5 / sqrt(w.asmthinv2)) : 0.0;
   double ax = 0, ay = 0, az = 0, pt = 0;
@@ -82,8 +119,10 @@ __global__ void __launch_bounds__(kTile) k_direct_noalloc(const double *__restri
       int64_t j = jb + threadIdx.x;
       if(j < j1)
         {
-          src[threadIdx.x]  = make_double4(pos[3 * j + 0], pos[3 * j + 1], pos[3 * j + 2], mass[j]);
-          hsrc[threadIdx.x] = w.soft[st[j]];
+          // a source without a softening length gets a NaN mass: every pair it enters is NaN
+          const double hj   = soft_of(w, st[j]);
+          src[threadIdx.x]  = make_double4(pos[3 * j + 0], pos[3 * j + 1], pos[3 * j + 2], hj == hj ? mass[j] : hj);
+          hsrc[threadIdx.x] = hj;
         }
       __syncthreads();
       int cnt = (int)((j1 - jb) < kTile ? (j1 - jb) : kTile);
@@ -179,8 +218,9 @@ extern "C" int32_t gpugrav_direct_noalloc(int32_t device, const gpugrav_params *
                                           const double *target_pos, const uint8_t *target_softtype, int32_t mode,
                                           double *acc, double *pot, void *stream)
 {
-  if(!params || params->abi_version != GPUGRAV_ABI_VERSION || params->nsofttypes < 1 ||
-     params->nsofttypes > GPUGRAV_MAX_SOFTTYPES || (params->periodic && !(params->asmth > 0)))
+  if(gg::validate_params(params) != GPUGRAV_OK)
+    return GPUGRAV_ERR_INVALID;
+  if(params->periodic && !(params->asmth > 0))  // the Ewald tables would need an allocation
     return GPUGRAV_ERR_INVALID;
   if(mode != GPUGRAV_DIRECT_FULL && mode != GPUGRAV_DIRECT_CUT)
     return GPUGRAV_ERR_INVALID;
@@ -188,7 +228,7 @@ extern "C" int32_t gpugrav_direct_noalloc(int32_t device, const gpugrav_params *
     return GPUGRAV_ERR_INVALID;
   if(ntargets > kMaxTargets)
     return GPUGRAV_ERR_TOO_LARGE;
-  if(device < 0 || device >= 64)
+  if(device < 0)
     return GPUGRAV_ERR_INVALID;
   if(ntargets == 0)
     return GPUGRAV_OK;
@@ -199,15 +239,29 @@ extern "C" int32_t gpugrav_direct_noalloc(int32_t device, const gpugrav_params *
   if(prev != device && cudaSetDevice(device) != cudaSuccess)
     return GPUGRAV_ERR_CUDA;
   int32_t status = GPUGRAV_OK;
-  // set-up, once per device with that device current: the device address of the scratch array
-  if(!g_partial_addr[device])
-    {
-      void *p = nullptr;
-      if(cudaGetSymbolAddress(&p, g_noalloc_partial) != cudaSuccess || !p)
-        status = GPUGRAV_ERR_CUDA;
-      else
-        g_partial_addr[device] = (double4 *)p;
-    }
+  // set-up, once per CUDA context with the device current: the device address of the scratch array
+  double4 *scratch = nullptr;
+  {
+    CtxGetCurrentFn get = ctx_get_current();
+    void *ctx           = nullptr;
+    if(!get || get(&ctx) != 0)
+      status = GPUGRAV_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    for(int i = 0; status == GPUGRAV_OK && i < g_scratch_n; i++)
+      if(g_scratch_addr[i].ctx == ctx)
+        scratch = g_scratch_addr[i].addr;
+    if(status == GPUGRAV_OK && !scratch)
+      {
+        void *p = nullptr;
+        if(g_scratch_n >= kMaxContexts || cudaGetSymbolAddress(&p, g_noalloc_partial) != cudaSuccess || !p)
+          status = GPUGRAV_ERR_CUDA;
+        else
+          {
+            g_scratch_addr[g_scratch_n++] = ScratchAddr{ctx, (double4 *)p};
+            scratch                       = (double4 *)p;
+          }
+      }
+  }
   if(status == GPUGRAV_OK)
     {
       gg::WalkConst wc;
@@ -215,8 +269,8 @@ extern "C" int32_t gpugrav_direct_noalloc(int32_t device, const gpugrav_params *
       cudaStream_t st = (cudaStream_t)stream;
       dim3 grid((unsigned)((ntargets + kTile - 1) / kTile), kChunks);
       k_direct_noalloc<<<grid, kTile, 0, st>>>(pos, mass, softtype, n, target_pos, target_softtype, ntargets, wc,
-                                               mode == GPUGRAV_DIRECT_CUT, g_partial_addr[device]);
-      k_direct_noalloc_reduce<<<(unsigned)((ntargets + 255) / 256), 256, 0, st>>>(g_partial_addr[device], ntargets, acc, pot);
+                                               mode == GPUGRAV_DIRECT_CUT, scratch);
+      k_direct_noalloc_reduce<<<(unsigned)((ntargets + 255) / 256), 256, 0, st>>>(scratch, ntargets, acc, pot);
       if(cudaGetLastError() != cudaSuccess)
         status = GPUGRAV_ERR_CUDA;
     }

@@ -118,36 +118,6 @@ int fail(gpugrav_ctx *c, int status, const char *what, cudaError_t e = cudaSucce
     }                                                  \
   while(0)
 
-int validate_params(const gpugrav_params *p)
-{
-  if(!p || p->abi_version != GPUGRAV_ABI_VERSION)
-    return GPUGRAV_ERR_INVALID;
-  if(p->nsofttypes < 1 || p->nsofttypes > GPUGRAV_MAX_SOFTTYPES)
-    return GPUGRAV_ERR_INVALID;
-  if(p->force_softening[p->nsofttypes] != 0.0)
-    return GPUGRAV_ERR_INVALID;
-  for(int i = 0; i < p->nsofttypes; i++)
-    if(!(p->force_softening[i] >= 0.0) || !std::isfinite(p->force_softening[i]))
-      return GPUGRAV_ERR_INVALID;
-  if(!(p->box_size > 0) || !std::isfinite(p->box_size))
-    return GPUGRAV_ERR_INVALID;
-  if(p->periodic && p->asmth != 0.0)
-    {
-      // TreePM split; asmth == 0 selects the pure periodic tree with Ewald correction
-      if(!(p->asmth > 0) || !(p->rcut > 0) || !(p->rcut_cells > 0))
-        return GPUGRAV_ERR_INVALID;
-    }
-  if(!(p->err_tol_theta >= 0) || !(p->err_tol_force_acc >= 0))
-    return GPUGRAV_ERR_INVALID;
-  if(p->precision != GPUGRAV_PREC_FP64 && p->precision != GPUGRAV_PREC_FP32)
-    return GPUGRAV_ERR_INVALID;
-  if(p->multiple_domains < 1 || p->multiple_domains > 512 || !(p->top_node_factor > 0))
-    return GPUGRAV_ERR_INVALID;
-  if((p->flags & ~GPUGRAV_FLAG_MULTIPLE_NODE_SOFTENING) != 0 || p->reserved != 0)
-    return GPUGRAV_ERR_INVALID;
-  return GPUGRAV_OK;
-}
-
 __global__ void k_gather_f32(const float *__restrict__ in, const uint32_t *__restrict__ perm, int64_t n, float *__restrict__ out)
 {
   for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -203,6 +173,37 @@ float elapsed(cudaEvent_t a, cudaEvent_t b)
   return ms;
 }
 }  // namespace
+
+// Parameter checks shared by every entry point that takes a gpugrav_params.
+int gg::validate_params(const gpugrav_params *p)
+{
+  if(!p || p->abi_version != GPUGRAV_ABI_VERSION)
+    return GPUGRAV_ERR_INVALID;
+  if(p->nsofttypes < 1 || p->nsofttypes > GPUGRAV_MAX_SOFTTYPES)
+    return GPUGRAV_ERR_INVALID;
+  if(p->force_softening[p->nsofttypes] != 0.0)
+    return GPUGRAV_ERR_INVALID;
+  for(int i = 0; i < p->nsofttypes; i++)
+    if(!(p->force_softening[i] >= 0.0) || !std::isfinite(p->force_softening[i]))
+      return GPUGRAV_ERR_INVALID;
+  if(!(p->box_size > 0) || !std::isfinite(p->box_size))
+    return GPUGRAV_ERR_INVALID;
+  if(p->periodic && p->asmth != 0.0)
+    {
+      // TreePM split; asmth == 0 selects the pure periodic tree with Ewald correction
+      if(!(p->asmth > 0) || !(p->rcut > 0) || !(p->rcut_cells > 0))
+        return GPUGRAV_ERR_INVALID;
+    }
+  if(!(p->err_tol_theta >= 0) || !(p->err_tol_force_acc >= 0))
+    return GPUGRAV_ERR_INVALID;
+  if(p->precision != GPUGRAV_PREC_FP64 && p->precision != GPUGRAV_PREC_FP32)
+    return GPUGRAV_ERR_INVALID;
+  if(p->multiple_domains < 1 || p->multiple_domains > 512 || !(p->top_node_factor > 0))
+    return GPUGRAV_ERR_INVALID;
+  if((p->flags & ~GPUGRAV_FLAG_MULTIPLE_NODE_SOFTENING) != 0 || p->reserved != 0)
+    return GPUGRAV_ERR_INVALID;
+  return GPUGRAV_OK;
+}
 
 // short-range table exactly as force_short_range_init (src/gravity/forcetree_walk.c:72-85)
 void gg::make_walk_const(const gpugrav_params &p, WalkConst *w)

@@ -269,4 +269,7 @@ cudaError_t layout32_stage(gpugrav_ctx *c);
 cudaError_t direct_stage(gpugrav_ctx *c, const WalkConst &wc, int64_t nt, const int64_t *d_targets, int cut, double *d_acc,
                          double *d_pot);
 void make_walk_const(const gpugrav_params &p, WalkConst *wc);
+// GPUGRAV_OK or GPUGRAV_ERR_INVALID: ABI version, softening table (finite, >= 0, zero end entry),
+// box size, TreePM split (asmth, rcut, rcut_cells > 0 unless asmth == 0), tolerances, flags
+int validate_params(const gpugrav_params *p);
 }  // namespace gg

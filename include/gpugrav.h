@@ -196,6 +196,10 @@ int32_t gpugrav_walk(gpugrav_ctx *ctx, const float *oldacc, double *acc, double 
  * sum exactly to the unsliced result. Default 0 of 1 (all targets). */
 int32_t gpugrav_set_target_slice(gpugrav_ctx *ctx, int32_t slice, int32_t nslices);
 
+/* Read-back of ExtNodes[].mass_per_type under MULTIPLE_NODE_SOFTENING: num_nodes x nsofttypes
+ * doubles in the reference's node order (parity checks). */
+int32_t gpugrav_export_mass_per_type(gpugrav_ctx *ctx, double *out);
+
 /* Periodic box without PM (params: periodic = 1, asmth = 0): the walks use the nearest image of
  * every node and particle plus the reference's Ewald correction per interaction
  * (src/gravity/forcetree_walk.c:469-477, forcetree_ewald.c:268-391). The correction tables are those
@@ -204,10 +208,6 @@ int32_t gpugrav_set_target_slice(gpugrav_ctx *ctx, int32_t slice, int32_t nslice
  * to box_size; a caller that already holds AREPO's tables (Ewd_fcorrx/y/z, Ewd_potcorr after
  * ewald_init, i.e. scaled to its box) passes them here: en = EN = 64, (en+1)^3 doubles each,
  * last index fastest. They are copied; they stay in use until the next call. */
-/* Read-back of ExtNodes[].mass_per_type under MULTIPLE_NODE_SOFTENING: num_nodes x nsofttypes
- * doubles in the reference's node order (parity checks). */
-int32_t gpugrav_export_mass_per_type(gpugrav_ctx *ctx, double *out);
-
 int32_t gpugrav_set_ewald_table(gpugrav_ctx *ctx, int32_t en, const double *fcorrx, const double *fcorry,
                                 const double *fcorrz, const double *potcorr);
 
@@ -320,8 +320,12 @@ int32_t gpugrav_serve_get_stats(gpugrav_serve *srv, gpugrav_serve_stats *stats);
  * acc (ntargets*3) and pot (ntargets or NULL). Launches on `stream` (a cudaStream_t, NULL = default)
  * and returns without synchronising. At most 4096 targets per call (GPUGRAV_ERR_TOO_LARGE beyond);
  * its scratch is a fixed 4 MiB device array per GPU, held until exit and shared by all calls: calls
- * that overlap on the GPU race. The first call on a device resolves the array's address; make it
- * before any stream capture. Allocates nothing (no cudaMalloc/cudaFree). */
+ * that overlap on the GPU race. The first call in a CUDA context (the device's primary context, or a
+ * caller's own context made current on `device`) resolves the array's address in that context; make it
+ * before any stream capture. Softening types must lie in [0, nsofttypes): a target of another type gets
+ * NaN outputs, and a source of another type makes every pair it enters NaN. The parameters are checked
+ * as gpugrav_create checks them; a periodic box needs asmth > 0 (the Ewald mode needs its tables, an
+ * allocation). Allocates nothing (no cudaMalloc/cudaFree). */
 int32_t gpugrav_direct_noalloc(int32_t device, const gpugrav_params *params, int64_t n, const double *pos,
                                const double *mass, const uint8_t *softtype, int64_t ntargets, const double *target_pos,
                                const uint8_t *target_softtype, int32_t mode, double *acc, double *pot, void *stream);
