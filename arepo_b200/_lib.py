@@ -165,6 +165,7 @@ _SIGS = {
     "gpugrav_load": (C.c_int32, [_P, C.c_int64, _P, _P, _P, C.c_int32, C.POINTER(Domain)]),
     "gpugrav_build": (C.c_int32, [_P, _P, C.c_int32]),
     "gpugrav_walk": (C.c_int32, [_P, _P, _P, _P, _P, C.c_int32]),
+    "gpugrav_walk_targets": (C.c_int32, [_P, C.c_int64, _P, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_set_target_slice": (C.c_int32, [_P, C.c_int32, C.c_int32]),
     "gpugrav_pm_periodic": (C.c_int32, [_P, C.c_int32, C.c_int64, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_set_ewald_table": (C.c_int32, [_P, C.c_int32, _P, _P, _P, _P]),

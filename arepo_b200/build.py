@@ -29,6 +29,7 @@ SOURCES = [
     ("direct.cu", True),
     ("direct_noalloc.cu", True),
     ("walk32.cu", False),
+    ("targets.cu", False),
     ("peak.cu", False),
     ("serve.cu", False),
     ("pm.cu", False),

@@ -349,7 +349,7 @@ int32_t gpugrav_destroy(gpugrav_ctx *c)
                         &c->nint_s, &c->oldacc_s, &c->oldacc_in, &c->out_acc, &c->out_pot, &c->out_nint, &c->scratch,
                         &c->g_groups, &c->g_ngroups, &c->g_gpd, &c->g_gseg, &c->g_gflag, &c->g_gid, &c->m_sys, &c->m_doms,
                         &c->pm_pos, &c->pm_mass, &c->pm_acc, &c->pm_pot, &c->ewd, &c->ewd32, &c->n_mpt, &c->w_mpt,
-                        &c->g_mpt};
+                        &c->g_mpt, &c->iperm, &c->t_in, &c->t_pos, &c->t_pos_alt, &c->t_idx, &c->t_idx_alt};
   gg::pm_release(c);
   for(auto *b : bufs)
     b->release();
@@ -614,20 +614,33 @@ int32_t gpugrav_set_target_slice(gpugrav_ctx *c, int32_t slice, int32_t nslices)
   return GPUGRAV_OK;
 }
 
-int32_t gpugrav_walk(gpugrav_ctx *c, const float *oldacc, double *acc, double *pot, int32_t *ninter, int32_t mem)
+}  // extern "C"
+
+namespace
+{
+// gravity_tree for every loaded particle (targets == nullptr) or for the caller's list of active
+// particles (caller indices); outputs in caller order or in the order of the list
+int walk_impl(gpugrav_ctx *c, int64_t nt, const int32_t *targets, const float *oldacc, double *acc, double *pot,
+              int32_t *ninter, int32_t mem)
 {
   if(!c)
     return GPUGRAV_ERR_INVALID;
   if(!c->built)
     return fail(c, GPUGRAV_ERR_STATE, "gpugrav_walk before gpugrav_build");
-  if(!acc || (mem != GPUGRAV_MEM_HOST && mem != GPUGRAV_MEM_DEVICE))
+  const bool active = targets != nullptr;
+  if((!acc && !(active && nt == 0)) || (mem != GPUGRAV_MEM_HOST && mem != GPUGRAV_MEM_DEVICE))
     return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_walk: acc must be non-null");
+  if(active && (nt < 0 || nt > c->n))
+    return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_walk_targets: need 0 <= ntargets <= n");
+  if(active && nt == 0)
+    return GPUGRAV_OK;
   DeviceGuard g(c->device);
   cudaStream_t st = c->stream;
-  const int64_t n = c->n;
+  const int64_t n    = c->n;
+  const int64_t nout = active ? nt : n;
   if(c->acc_s.ensure(n * 3 * sizeof(double)) != cudaSuccess || c->pot_s.ensure(n * sizeof(double)) != cudaSuccess ||
      c->nint_s.ensure(n * sizeof(int32_t)) != cudaSuccess || c->oldacc_s.ensure(n * sizeof(float)) != cudaSuccess ||
-     c->oldacc_in.ensure(n * sizeof(float)) != cudaSuccess)
+     c->oldacc_in.ensure(n * sizeof(float)) != cudaSuccess || (active && c->t_in.ensure(nt * sizeof(int32_t) + 16) != cudaSuccess))
     return fail(c, GPUGRAV_ERR_OOM, "gpugrav_walk: device allocation");
   WalkConst wc;
   make_walk_const(c->prm, &wc);
@@ -653,40 +666,107 @@ int32_t gpugrav_walk(gpugrav_ctx *c, const float *oldacc, double *acc, double *p
         old_dev = oldacc;
     }
   k_gather_f32<<<grid_for(n, 256), 256, 0, st>>>(old_dev, c->perm.as<uint32_t>(), n, c->oldacc_s.as<float>());
+  // active list: sorted positions in key order (targets_stage checks range and duplicates)
+  const bool fp32 = c->prm.precision == GPUGRAV_PREC_FP32;
+  const int cap   = 32 * ((c->walk32_tpl == 1 || c->multi || wc.ewald) ? 1 : 2);  // FP32 group size
+  int64_t a = 0, b = nout;  // this call's target slice of the active list
+  c->w_tlist    = nullptr;
+  c->w_ntargets = 0;
+  if(active)
+    {
+      const int32_t *d_t = targets;
+      if(mem == GPUGRAV_MEM_HOST)
+        {
+          CK(cudaMemcpyAsync(c->t_in.p, targets, nt * sizeof(int32_t), cudaMemcpyHostToDevice, st), "upload targets");
+          d_t = c->t_in.as<int32_t>();
+        }
+      int flags = 0;
+      CK(gg::targets_stage(c, nt, d_t, &flags), "active targets");
+      if(flags & 1)
+        return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_walk_targets: target index outside [0, n)");
+      if(flags & 2)
+        return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_walk_targets: a particle is listed twice");
+      if(fp32)
+        {
+          const int64_t ng = (nt + cap - 1) / cap, gb = ng * c->slice / c->nslices, ge = ng * (c->slice + 1) / c->nslices;
+          a = gb * cap;
+          b = ge * cap < nt ? ge * cap : nt;
+        }
+      else
+        {
+          a = nt * c->slice / c->nslices;
+          b = nt * (c->slice + 1) / c->nslices;
+        }
+    }
   CK(cudaMemsetAsync(c->counters.as<int>() + 32, 0, 8, st), "reset counters");
   CK(cudaMemsetAsync(c->counters.as<int>() + 14, 0, 4, st), "reset counters");
   cudaEventRecord(c->ev[8], st);
-  if(c->prm.precision == GPUGRAV_PREC_FP32)
+  cudaError_t we = cudaSuccess;
+  if(fp32)
     {
-      CK(gg::walk32_stage(c, wc), "fp32 walk");
+      we = gg::walk32_prepare(c, wc);
+      if(we == cudaSuccess)
+        {
+          if(active)
+            {
+              we               = gg::groups_active_stage(c, nt, cap);
+              c->groups_active = true;
+            }
+          else if(c->groups_active)
+            {
+              we               = gg::groups_stage(c);  // the table of every particle again
+              c->groups_active = false;
+            }
+        }
+      if(active)
+        {
+          c->w_tlist    = c->t_pos_alt.as<int32_t>();
+          c->w_ntargets = nt;
+        }
+      if(we == cudaSuccess)
+        we = gg::walk32_launch(c);
     }
   else
     {
-      CK(gg::walk64_stage(c, wc), "fp64 walk");
+      if(active)
+        {
+          c->w_tlist    = c->t_pos_alt.as<int32_t>();
+          c->w_ntargets = nt;
+        }
+      we = gg::walk64_stage(c, wc);
     }
-  CK(gg::slice_mask_stage(c, c->prm.precision == GPUGRAV_PREC_FP32), "target slice");
+  c->w_tlist    = nullptr;
+  c->w_ntargets = 0;
+  CK(we, fp32 ? "fp32 walk" : "fp64 walk");
+  if(!active)
+    CK(gg::slice_mask_stage(c, fp32), "target slice");
   cudaEventRecord(c->ev[9], st);
   double *d_acc = acc, *d_pot = pot;
   int32_t *d_nint = ninter;
   if(mem == GPUGRAV_MEM_HOST)
     {
-      if(c->out_acc.ensure(n * 3 * sizeof(double)) != cudaSuccess || c->out_pot.ensure(n * sizeof(double)) != cudaSuccess ||
-         c->out_nint.ensure(n * sizeof(int32_t)) != cudaSuccess)
+      if(c->out_acc.ensure(nout * 3 * sizeof(double)) != cudaSuccess || c->out_pot.ensure(nout * sizeof(double)) != cudaSuccess ||
+         c->out_nint.ensure(nout * sizeof(int32_t)) != cudaSuccess)
         return fail(c, GPUGRAV_ERR_OOM, "gpugrav_walk: output staging");
       d_acc  = c->out_acc.as<double>();
       d_pot  = pot ? c->out_pot.as<double>() : nullptr;
       d_nint = ninter ? c->out_nint.as<int32_t>() : nullptr;
     }
-  k_scatter_out<<<grid_for(n, 256), 256, 0, st>>>(c->acc_s.as<double>(), c->pot_s.as<double>(), c->nint_s.as<int32_t>(),
-                                                  c->perm.as<uint32_t>(), n, d_acc, d_pot, d_nint);
-  CK(cudaGetLastError(), "scatter");
+  if(active)
+    CK(gg::targets_scatter(c, nt, a, b, d_acc, d_pot, d_nint), "scatter");
+  else
+    {
+      k_scatter_out<<<grid_for(n, 256), 256, 0, st>>>(c->acc_s.as<double>(), c->pot_s.as<double>(), c->nint_s.as<int32_t>(),
+                                                      c->perm.as<uint32_t>(), n, d_acc, d_pot, d_nint);
+      CK(cudaGetLastError(), "scatter");
+    }
   if(mem == GPUGRAV_MEM_HOST)
     {
-      CK(cudaMemcpyAsync(acc, d_acc, n * 3 * sizeof(double), cudaMemcpyDeviceToHost, st), "download acc");
+      CK(cudaMemcpyAsync(acc, d_acc, nout * 3 * sizeof(double), cudaMemcpyDeviceToHost, st), "download acc");
       if(pot)
-        CK(cudaMemcpyAsync(pot, d_pot, n * sizeof(double), cudaMemcpyDeviceToHost, st), "download pot");
+        CK(cudaMemcpyAsync(pot, d_pot, nout * sizeof(double), cudaMemcpyDeviceToHost, st), "download pot");
       if(ninter)
-        CK(cudaMemcpyAsync(ninter, d_nint, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "download interactions");
+        CK(cudaMemcpyAsync(ninter, d_nint, nout * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "download interactions");
     }
   unsigned long long tot = 0;
   int walk_err = 0;
@@ -701,6 +781,23 @@ int32_t gpugrav_walk(gpugrav_ctx *c, const float *oldacc, double *acc, double *p
   c->timings.interactions         = (int64_t)tot;
   c->timings.walk_kernel_launches = 1;
   return GPUGRAV_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int32_t gpugrav_walk(gpugrav_ctx *c, const float *oldacc, double *acc, double *pot, int32_t *ninter, int32_t mem)
+{
+  return walk_impl(c, 0, nullptr, oldacc, acc, pot, ninter, mem);
+}
+
+int32_t gpugrav_walk_targets(gpugrav_ctx *c, int64_t ntargets, const int32_t *targets, const float *oldacc, double *acc,
+                             double *pot, int32_t *ninter, int32_t mem)
+{
+  if(!targets && ntargets != 0)
+    return c ? fail(c, GPUGRAV_ERR_INVALID, "gpugrav_walk_targets: targets is null") : GPUGRAV_ERR_INVALID;
+  static const int32_t none = 0;
+  return walk_impl(c, ntargets, targets ? targets : &none, oldacc, acc, pot, ninter, mem);
 }
 
 int32_t gpugrav_compute(gpugrav_ctx *c, int64_t n, const double *pos, const double *mass, const uint8_t *softtype,

@@ -213,6 +213,12 @@ struct gpugrav_ctx
   gg::DevBuf g_groups, g_ngroups;             // walk groups (first, count, root, criterion), their count
   gg::DevBuf g_gpd, g_gseg, g_gflag, g_gid;   // group construction scratch
   int32_t slice = 0, nslices = 1;             // target slice of the walks (gpugrav_set_target_slice)
+  // active targets of the current walk (gpugrav_walk_targets): sorted particle positions in key order
+  // (t_pos_alt) and their places in the caller's list (t_idx_alt); w_tlist is null for a walk of every particle
+  gg::DevBuf iperm, t_in, t_pos, t_pos_alt, t_idx, t_idx_alt;
+  const int32_t *w_tlist = nullptr;
+  int64_t w_ntargets     = 0;
+  bool groups_active     = false;  // the FP32 group table describes an active list, not every particle
   // Ewald correction tables (ewald.cu): FP64 and float4 copies, scaled to ewd_box (or the caller's)
   gg::DevBuf ewd, ewd32;
   double ewd_box = 0;
@@ -254,6 +260,9 @@ cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc);
 cudaError_t walk32_prepare(gpugrav_ctx *c, const WalkConst &wc);
 cudaError_t walk32_launch(gpugrav_ctx *c);
 cudaError_t groups_stage(gpugrav_ctx *c);
+cudaError_t targets_stage(gpugrav_ctx *c, int64_t nt, const int32_t *d_targets, int *flags);
+cudaError_t groups_active_stage(gpugrav_ctx *c, int64_t nt, int cap);
+cudaError_t targets_scatter(gpugrav_ctx *c, int64_t nt, int64_t a, int64_t b, double *acc, double *pot, int32_t *nint);
 cudaError_t slice_mask_stage(gpugrav_ctx *c, bool fp32);
 const std::vector<double> &ewald_unit_table();
 cudaError_t ewald_upload(gpugrav_ctx *c, const double *user);

@@ -45,8 +45,12 @@ constexpr int kUnroll  = GG_W32_UNROLL;   // list entries in flight per lane in 
 #define GG_W32_MINBLOCKS 5  // blocks per SM the register budget is sized for (96 registers a thread)
 #endif
 // capacity: accepted nodes (<= 32) join a list holding fewer than kEvalAt entries; particles are
-// added at most 32 per round and the list is evaluated first whenever a round could overflow it
+// added at most 32 per round and the list is evaluated first whenever a round could overflow it.
+// Entries inside some target's softening length go to a separate, smaller near list, evaluated as
+// soon as it holds kNearAt entries.
 constexpr int kListCap = kEvalAt + 64;
+constexpr int kNearAt  = 64;
+constexpr int kNearCap = kNearAt + 64;
 constexpr int kStackCap = 16384;  // traversal stack entries per warp (global memory)
 // A node that the group-box test opens although it is smaller than 1/kVote of the box's largest side
 // and nearer to the box than that is tested against every target of the group instead (opened
@@ -77,7 +81,8 @@ constexpr float kVote = 16.0f;
 struct W32Const
 {
   double box, half_box;
-  float rcut, rcut2, asmthfac, pad1;
+  float rcut, rcut2, asmthfac;
+  float rcut2_all;  // an entry whose farthest distance from the group box is below this is inside Rcut of every target
   float theta2, erracc;
   int periodic, bh;
   float soft[GPUGRAV_MAX_SOFTTYPES + 1];
@@ -220,11 +225,14 @@ __device__ __forceinline__ float rsqrt_normal(float x)
 // Short-range factors of the TreePM split at separation r: linear interpolation of the force
 // (scaled by 1/Asmth^2) and potential tables between nodes floor(te) and floor(te) + 1,
 // te = r * asmthfac, as the reference does (src/gravity/forcetree_walk.c:366-379).  Adding 1.5 * 2^23 with rounding toward minus
-// infinity leaves floor(te) in the low mantissa bits (no conversion instruction); the index is
-// clamped to the last interval, which only entries beyond Rcut reach (they are masked).
+// infinity leaves floor(te) in the low mantissa bits (no conversion instruction).  CLAMP: the index
+// is clamped to the last interval, which only entries beyond Rcut reach (they are masked); without
+// CLAMP the entry is inside Rcut, so floor(te) <= NTAB (the table has NTAB + 1 rows).
+template <bool CLAMP = true>
 __device__ __forceinline__ void short_range(float r, const W32Const &w, float &ff, float &fpt)
 {
-  const float tb0 = fminf(__fmaf_rd(r, w.asmthfac, 12582912.0f), 12582912.0f + (float)(kNtab - 1));
+  const float tr  = __fmaf_rd(r, w.asmthfac, 12582912.0f);
+  const float tb0 = CLAMP ? fminf(tr, 12582912.0f + (float)(kNtab - 1)) : tr;
   const float tw  = fmaf(r, w.asmthfac, 12582912.0f - tb0);
   const float4 t  = w.tab[__float_as_int(tb0) - 0x4B400000];
   ff              = fmaf(tw, t.y, t.x);
@@ -287,24 +295,27 @@ __device__ __forceinline__ Sep separation(const float4 e, const Tgt &T)
 }
 
 // One target against one list entry, outside the softening length (r >= max(h_i, h_j)): the
-// Newtonian kernel, times the TreePM short-range factor when PERIODIC.  An entry beyond Rcut of this
-// target (periodic) is masked, not branched around, so that the interactions of an unrolled block
-// schedule together.  CHECK: the entry may lie inside the softening length of this target; such a
-// pair is masked as well and reported by the return value, and near() adds the spline kernel for
-// it.  Without CHECK the list entry is known to lie outside the softening length of every target
-// of the group.  The interaction count and the Ewald correction (EWALD: pure periodic tree, nearest
-// image) are taken here for every pair.
-template <bool PERIODIC, bool POT, bool EWALD = false, bool CHECK = true>
+// Newtonian kernel, times the TreePM short-range factor when PERIODIC.  MASK: an entry beyond Rcut
+// of this target (periodic) is masked, not branched around, so that the interactions of an unrolled
+// block schedule together, and the pair is counted only inside Rcut; without MASK the entry is known
+// to lie inside Rcut of every target of the group and its interactions are counted per list region.
+// CHECK: the entry may lie inside the softening length of this target; such a pair is masked as well
+// and reported by the return value, and near() adds the spline kernel for it.  Without CHECK the list
+// entry is known to lie outside the softening length of every target of the group.  The Ewald
+// correction (EWALD: pure periodic tree, nearest image) is taken here for every pair.
+template <bool PERIODIC, bool POT, bool EWALD = false, bool CHECK = true, bool MASK = true>
 __device__ __forceinline__ bool far(const float4 e, const float hj, Tgt &T, const W32Const &w)
 {
+  constexpr bool PAIRWISE = MASK || CHECK;  // Rcut mask and count per pair
   // outside every target's softening length (no CHECK) r > 0 unless the softening is zero
   const Sep s = separation<CHECK>(e, T);
   bool in     = true;
   float ff = 0.0f, fpt = 0.0f;
   if(PERIODIC)
     {
-      in = s.r2 < w.rcut2;
-      short_range(s.r, w, ff, fpt);
+      if(PAIRWISE)
+        in = s.r2 < w.rcut2;
+      short_range<PAIRWISE>(s.r, w, ff, fpt);
     }
   // force m (1/r^3 + f_s / (r Asmth^2)) = (m/r) (1/r^2 + f_s'), potential (m/r) p_s (Newtonian: -m/r);
   // 1/r^2 stays finite at the clamped r = 0, so masking m/r masks both
@@ -326,7 +337,8 @@ __device__ __forceinline__ bool far(const float4 e, const float hj, Tgt &T, cons
       if(POT)
         T.pot = fmaf(m, c.w, T.pot);
     }
-  T.ni += in ? 1 : 0;  // list entries all have mass != 0
+  if(PAIRWISE)
+    T.ni += in ? 1 : 0;  // list entries all have mass != 0
   return soft;
 }
 
@@ -383,8 +395,8 @@ __device__ __forceinline__ void near(const float4 e, const float hj, Tgt &T, con
 #ifdef GG_WALK32_STATS
 }  // namespace
 // measurement build only: [0] list entries evaluated per lane, [1] node tests, [2] particle candidates,
-// [3] groups
-__device__ unsigned long long g_walk_stats[4];
+// [3] groups, [4] entries inside Rcut of every target, [5] border entries, [6] warp steps
+__device__ unsigned long long g_walk_stats[8];
 namespace
 {
 #define WALK_STAT(i, v)                       \
@@ -402,13 +414,11 @@ namespace
   while(0)
 #endif
 
-// The lane's TPL targets against the warp's list (each entry read once for all of them), in blocks
-// of kUnroll entries evaluated without branches.  The list has two regions: `nf` far entries at the
-// bottom of the buffer, outside the softening length of every target of the group, and `nn` near
-// entries at the top, for which a block in which some pair lies inside the softening length (the
-// targets' own particles, close neighbours) is revisited for those pairs.  Then the batch partials
-// are folded into the FP64 sums.
-template <bool PERIODIC, bool POT, int TPL, bool EWALD, bool CHECK>
+// The lane's TPL targets against one region of the warp's list (each entry read once for all of
+// them), in blocks of kUnroll entries evaluated without branches.  CHECK (near list): a block in
+// which some pair lies inside the softening length (the targets' own particles, close neighbours)
+// is revisited for those pairs.  MASK: per-pair Rcut mask and count (see far()).
+template <bool PERIODIC, bool POT, int TPL, bool EWALD, bool CHECK, bool MASK>
 __device__ __forceinline__ void evaluate_region(const float4 *__restrict__ LP, const float *__restrict__ LH, int nl, Tgt (&T)[TPL],
                                                 const W32Const &w)
 {
@@ -421,14 +431,14 @@ __device__ __forceinline__ void evaluate_region(const float4 *__restrict__ LP, c
       for(int u = 0; u < kUnroll; u++)
         {
           e[u]  = LP[j + u];
-          hj[u] = LH[j + u];
+          hj[u] = CHECK ? LH[j + u] : 0.0f;
         }
       bool soft = false;
 #pragma unroll
       for(int u = 0; u < kUnroll; u++)
 #pragma unroll
         for(int k = 0; k < TPL; k++)
-          soft |= far<PERIODIC, POT, EWALD, CHECK>(e[u], hj[u], T[k], w);
+          soft |= far<PERIODIC, POT, EWALD, CHECK, MASK>(e[u], hj[u], T[k], w);
       if(CHECK && soft)
         {
 #pragma unroll 1
@@ -445,45 +455,88 @@ __device__ __forceinline__ void evaluate_region(const float4 *__restrict__ LP, c
   for(; j < nl; j++)
     {
       const float4 e = LP[j];
-      const float hj = LH[j];
+      const float hj = CHECK ? LH[j] : 0.0f;
 #pragma unroll
       for(int k = 0; k < TPL; k++)
-        if(far<PERIODIC, POT, EWALD, CHECK>(e, hj, T[k], w) && CHECK)
+        if(far<PERIODIC, POT, EWALD, CHECK, MASK>(e, hj, T[k], w) && CHECK)
           near<PERIODIC, POT>(e, hj, T[k], w);
     }
 }
 
-template <bool PERIODIC, bool POT, int TPL, bool EWALD = false>
-__device__ __forceinline__ void evaluate(const float4 *__restrict__ LP, const float *__restrict__ LH, int nf, int nn, Tgt (&T)[TPL],
-                                         const W32Const &w)
+// The warp's interaction list in shared memory.  Main buffer: entries outside the softening length of
+// every target of the group, those inside Rcut of every target at the bottom (growing up, `na`),
+// the others at the top (growing down, `nb`).  Near buffer (`nn`): entries inside some target's
+// softening length, with their softening lengths.
+struct List
 {
-  evaluate_region<PERIODIC, POT, TPL, EWALD, false>(LP, LH, nf, T, w);
-  evaluate_region<PERIODIC, POT, TPL, EWALD, true>(LP + kListCap - nn, LH + kListCap - nn, nn, T, w);
+  float4 *P;
+  float4 *NP;
+  float *NH;
+  int na, nb, nn;
+};
+
+// Evaluates and empties the list, then folds the batch partials into the FP64 sums.
+template <bool PERIODIC, bool POT, int TPL, bool EWALD = false>
+__device__ __forceinline__ void evaluate(List &L, Tgt (&T)[TPL], const W32Const &w)
+{
+  WALK_STAT(4, L.na);
+  WALK_STAT(5, L.nb);
+  evaluate_region<PERIODIC, POT, TPL, EWALD, false, false>(L.P, nullptr, L.na, T, w);
+  evaluate_region<PERIODIC, POT, TPL, EWALD, false, true>(L.P + kListCap - L.nb, nullptr, L.nb, T, w);
+  evaluate_region<PERIODIC, POT, TPL, EWALD, true, true>(L.NP, L.NH, L.nn, T, w);
 #pragma unroll
   for(int k = 0; k < TPL; k++)
     {
+      T[k].ni += L.na;
       T[k].dax += T[k].ax;
       T[k].day += T[k].ay;
       T[k].daz += T[k].az;
       T[k].dpot += T[k].pot;
       T[k].ax = T[k].ay = T[k].az = T[k].pot = 0.0f;
     }
+  L.na = L.nb = L.nn = 0;
 }
 
-// Appends one entry per lane that keeps one to the warp's list: to the far region (bottom, growing
-// up) or, `nr`, to the near region (top, growing down).
-__device__ __forceinline__ void push(float4 *LP, float *LH, int &nf, int &nn, bool keep, bool nr, const float4 e, float h,
-                                     unsigned lt_mask)
+// true when a push round of up to 32 entries could overflow a buffer
+__device__ __forceinline__ bool list_full(const List &L) { return L.na + L.nb + 32 > kListCap || L.nn + 32 > kNearCap; }
+
+// Appends one entry per lane that keeps one to the warp's list.  The entry (x, y, z relative to the
+// group centre, mass) lies at squared distance d2 from the nearest point of the group box (half
+// extents bx, by, bz); hn is the larger of the group's largest softening (with margin) and the
+// entry's own.  Closer than hn: near list.  Otherwise, when its farthest distance from the box is
+// below Rcut (with margin) or there is no Rcut: inside Rcut of every target; else the border region.
+template <bool PERIODIC>
+__device__ __forceinline__ void push(List &L, bool keep, const float4 e, float h, float d2, float hn, float bx, float by, float bz,
+                                     const W32Const &w, unsigned lt_mask)
 {
-  const unsigned kf = __ballot_sync(0xffffffffu, keep && !nr), kn = __ballot_sync(0xffffffffu, keep && nr);
+  int cls = 2;
+  if(!(d2 < hn * hn))
+    {
+      cls = 0;
+      if(PERIODIC)
+        {
+          const float fx = fabsf(e.x) + bx, fy = fabsf(e.y) + by, fz = fabsf(e.z) + bz;
+          cls = (fmaf(fx, fx, fmaf(fy, fy, fz * fz)) < w.rcut2_all) ? 0 : 1;
+        }
+    }
+  const unsigned ka = __ballot_sync(0xffffffffu, keep && cls == 0), kb = __ballot_sync(0xffffffffu, keep && cls == 1),
+                 kn = __ballot_sync(0xffffffffu, keep && cls == 2);
   if(keep)
     {
-      const int pos = nr ? kListCap - 1 - (nn + __popc(kn & lt_mask)) : nf + __popc(kf & lt_mask);
-      LP[pos]       = e;
-      LH[pos]       = h;
+      if(cls == 0)
+        L.P[L.na + __popc(ka & lt_mask)] = e;
+      else if(cls == 1)
+        L.P[kListCap - 1 - (L.nb + __popc(kb & lt_mask))] = e;
+      else
+        {
+          const int q = L.nn + __popc(kn & lt_mask);
+          L.NP[q]     = e;
+          L.NH[q]     = h;
+        }
     }
-  nf += __popc(kf);
-  nn += __popc(kn);
+  L.na += __popc(ka);
+  L.nb += __popc(kb);
+  L.nn += __popc(kn);
 }
 
 template <bool PERIODIC, bool POT, int TPL, bool EWALD = false>
@@ -492,7 +545,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                                                         const uint8_t *__restrict__ g_pst, const double4 *__restrict__ tpm,
                                                         const uint8_t *__restrict__ tst, const float *__restrict__ oldacc,
                                                         const int *__restrict__ ngroups_dev, const int4 *__restrict__ groups,
-                                                        int slice, int nslices,
+                                                        const int32_t *__restrict__ tlist, int slice, int nslices,
                                                         const W32Const *__restrict__ wcp,
                                                         int *__restrict__ stack_base, int *__restrict__ work,
                                                         double *__restrict__ acc_out, double *__restrict__ pot_out,
@@ -501,7 +554,8 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
 {
   __shared__ W32Const w;
   __shared__ float4 il_p[kWarps][kListCap];
-  __shared__ float il_h[kWarps][kListCap];
+  __shared__ float4 il_np[kWarps][kNearCap];
+  __shared__ float il_nh[kWarps][kNearCap];
   for(int t = threadIdx.x; t < (int)(sizeof(W32Const) / 4); t += blockDim.x)
     ((int *)&w)[t] = ((const int *)wcp)[t];
   __syncthreads();
@@ -510,8 +564,10 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
   const int lane         = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
   int *stack             = stack_base + ((int64_t)blockIdx.x * kWarps + warp) * kStackCap;
-  float4 *LP             = il_p[warp];
-  float *LH              = il_h[warp];
+  List L;
+  L.P  = il_p[warp];
+  L.NP = il_np[warp];
+  L.NH = il_nh[warp];
   unsigned long long my_total = 0;
   // groups of this target slice; the count lives on the device (no host round trip, graph replays)
   const int64_t ng       = *ngroups_dev;
@@ -540,7 +596,9 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
       for(int k = 0; k < TPL; k++)
         {
           const int s      = lane + 32 * k;
-          const int64_t tt = t0 + (s < cnt ? s : 0);  // idle slots repeat the group's first target
+          // idle slots repeat the group's first target; a group of active targets (tlist) holds
+          // consecutive entries of the active list
+          const int64_t tt = tlist ? (int64_t)tlist[t0 + (s < cnt ? s : 0)] : t0 + (s < cnt ? s : 0);
           p[k]             = tpm[tt];
           a_l[k]           = w.erracc * oldacc[tt];
           mnx = fmin(mnx, p[k].x), mxx = fmax(mxx, p[k].x);
@@ -568,34 +626,111 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
       for(int k = 0; k < TPL; k++)
         {
           T[k].x = (float)(p[k].x - gx), T[k].y = (float)(p[k].y - gy), T[k].z = (float)(p[k].z - gz);
-          T[k].h  = w.soft[tst[t0 + (lane + 32 * k < cnt ? lane + 32 * k : 0)]];
+          const int sk = lane + 32 * k < cnt ? lane + 32 * k : 0;
+          T[k].h       = w.soft[tst[tlist ? (int64_t)tlist[t0 + sk] : t0 + sk]];
           T[k].ax = T[k].ay = T[k].az = T[k].pot = 0.0f;
           T[k].dax = T[k].day = T[k].daz = T[k].dpot = 0.0;
           T[k].ni = 0;
         }
 
-      int nf = 0, nn = 0, sp = 1;  // list: far and near entries
+      int sp = 1;
+      L.na = L.nb = L.nn = 0;
       if(lane == 0)
         stack[0] = root;
       __syncwarp();
 
-      while(sp > 0)
+      // The walk is a loop over warp-uniform work items, so that the list evaluation has a single
+      // (inlined) site: a pending softening-type entry of MULTIPLE_NODE_SOFTENING nodes (t_next <
+      // t_end), a pending round of up to 32 particles of opened nodes (q0 < ptot), or a step over
+      // up to 32 stack nodes.  The list is evaluated first when the next item could overflow it,
+      // when it is full enough at a node step, and at the end.
+      int t_next = 0, t_end = 0;  // MULTIPLE_NODE_SOFTENING entries of the last node step
+      int q0 = 0, ptot = 0;       // particle rounds of the last node step
+      // per-lane state of the last node step, read by the pending items
+      int node = -1, action = 0, fp = 0, pinc = 0, pexc = 0;
+      bool split = false;
+      float4 entry = make_float4(0, 0, 0, 0);
+      float ent_d2 = 0.0f;  // squared distance of the entry from the group box
+      while(true)
         {
+          const int queued = L.na + L.nb + L.nn;
+          const bool flush = (t_next < t_end || q0 < ptot) ? list_full(L)
+                                                           : (sp > 0 ? (queued >= kEvalAt || L.nn >= kNearAt) : queued > 0);
+          if(flush)
+            {
+              WALK_STAT(0, queued);
+              evaluate<PERIODIC, POT, TPL, EWALD>(L, T, w);
+              __syncwarp();
+            }
+          if(t_next < t_end)
+            {
+              // MULTIPLE_NODE_SOFTENING: one entry per softening type with that type's mass and softening
+              // (forcetree_walk.c:382-401); for a target whose own softening exceeds the node's largest
+              // this equals the single entry, the kernel being linear in the mass
+              const int t    = t_next++;
+              const float mt = (action == 1 && split) ? w.mpt[(int64_t)node * w.nsoft + t] : 0.0f;
+              push<PERIODIC>(L, mt != 0.0f, make_float4(entry.x, entry.y, entry.z, mt), w.soft[t], ent_d2,
+                             fmaxf(h_grp, w.soft[t]), ex, ey, ez, w, lt_mask);
+              continue;
+            }
+          if(q0 < ptot)
+            {
+              // particles of opened nodes -> list, one particle per lane per round; particles beyond
+              // Rcut of the whole group are dropped
+              const int q = q0 + lane;
+              q0 += 32;
+              int owner = 0;  // owner lane: number of lanes whose inclusive prefix is <= q
+#pragma unroll
+              for(int s = 16; s >= 1; s >>= 1)
+                {
+                  const int v = __shfl_sync(0xffffffffu, pinc, owner + s - 1);
+                  if(v <= q)
+                    owner += s;
+                }
+              owner          = owner < 31 ? owner : 31;
+              const int ofp  = __shfl_sync(0xffffffffu, fp, owner);
+              const int oexc = __shfl_sync(0xffffffffu, pexc, owner);
+              bool keep      = false;
+              float4 pe      = make_float4(0, 0, 0, 0);
+              float ph = 0, pd2 = 0;
+              if(q < ptot)
+                {
+                  const int pi     = ofp + (q - oexc);
+                  const double4 pp = g_pm[pi];
+                  pe = make_float4((float)wrapd(pp.x - gx, w), (float)wrapd(pp.y - gy, w), (float)wrapd(pp.z - gz, w),
+                                   (float)pp.w);
+                  ph   = w.soft[g_pst[pi]];
+                  keep = pp.w != 0.0;
+                  const float dmx = fmaxf(fabsf(pe.x) - ex, 0.0f), dmy = fmaxf(fabsf(pe.y) - ey, 0.0f),
+                              dmz = fmaxf(fabsf(pe.z) - ez, 0.0f);
+                  pd2 = dmx * dmx + dmy * dmy + dmz * dmz;
+                  if(PERIODIC)
+                    keep = keep && pd2 < w.rcut2;
+                }
+              push<PERIODIC>(L, keep, pe, ph, pd2, fmaxf(h_grp, ph), ex, ey, ez, w, lt_mask);
+              continue;
+            }
+          if(sp == 0)
+            break;
+
+          // ---- node step: up to 32 stack nodes, one per lane ----
           const int take = sp < 32 ? sp : 32;
           sp -= take;
           WALK_STAT(1, take);
-          int node = -1;
+          WALK_STAT(6, 1);
+          node = -1;
           if(lane < take)
             node = stack[sp + lane];
           __syncwarp();
 
-          int action = 0;  // 1 accept, 2 open
-          float4 entry = make_float4(0, 0, 0, 0);
-          float hj     = 0;
-          int fc = 0, fp = 0, nc = 0, np = 0;
-          float ent_d2 = 0.0f;  // squared distance of the entry from the group box
+          action = 0;  // 1 accept, 2 open
+          entry  = make_float4(0, 0, 0, 0);
+          ent_d2 = 0.0f;
+          split  = false;  // MULTIPLE_NODE_SOFTENING: accepted node listed per type
+          float hj = 0;
+          int fc = 0, nc = 0, np = 0;
+          fp = 0;
           bool vote = false, vote_keep = false;  // per-target vote pending; entry kept if accepted
-          bool split = false;                    // MULTIPLE_NODE_SOFTENING: accepted node listed per type
           float4 vrel = make_float4(0, 0, 0, 0);   // centre - CoM, side of a voting node
           if(node >= 0)
             {
@@ -698,75 +833,18 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                   nc = np = 0;
                 }
             }
-          // accepted nodes -> list (nodes used per softening type follow below)
-          {
-            const float hn = fmaxf(h_grp, hj);
-            push(LP, LH, nf, nn, action == 1 && !split, ent_d2 < hn * hn, entry, hj, lt_mask);
-          }
-          // MULTIPLE_NODE_SOFTENING: one entry per softening type with that type's mass and softening
-          // (forcetree_walk.c:382-401); for a target whose own softening exceeds the node's largest
-          // this equals the single entry, the kernel being linear in the mass
-          if(__ballot_sync(0xffffffffu, action == 1 && split))
-            for(int t = 0; t < w.nsoft; t++)
-              {
-                if(nf + nn + 32 > kListCap)
-                  {
-                    evaluate<PERIODIC, POT, TPL, EWALD>(LP, LH, nf, nn, T, w);
-                    nf = nn = 0;
-                    __syncwarp();
-                  }
-                const float mt = (action == 1 && split) ? w.mpt[(int64_t)node * w.nsoft + t] : 0.0f;
-                const float hn = fmaxf(h_grp, w.soft[t]);
-                push(LP, LH, nf, nn, mt != 0.0f, ent_d2 < hn * hn, make_float4(entry.x, entry.y, entry.z, mt), w.soft[t],
-                     lt_mask);
-              }
-          // particles of opened nodes -> list, one particle per lane per round; particles beyond
-          // Rcut of the whole group are dropped
-          const int npx  = (action == 2) ? np : 0;
-          const int pinc = wscan_incl(npx, lane);
-          const int ptot = __shfl_sync(0xffffffffu, pinc, 31);
-          const int pexc = pinc - npx;
+          // accepted nodes -> list (the list holds fewer than kEvalAt entries, so 32 more fit);
+          // nodes used per softening type follow as pending items
+          push<PERIODIC>(L, action == 1 && !split, entry, hj, ent_d2, fmaxf(h_grp, hj), ex, ey, ez, w, lt_mask);
+          t_next = 0;
+          t_end  = __ballot_sync(0xffffffffu, action == 1 && split) ? w.nsoft : 0;
+          // particles of opened nodes: pending rounds
+          const int npx = (action == 2) ? np : 0;
+          pinc          = wscan_incl(npx, lane);
+          ptot          = __shfl_sync(0xffffffffu, pinc, 31);
+          pexc          = pinc - npx;
+          q0            = 0;
           WALK_STAT(2, ptot);
-          for(int q0 = 0; q0 < ptot; q0 += 32)
-            {
-              if(nf + nn + 32 > kListCap)
-                {
-                  evaluate<PERIODIC, POT, TPL, EWALD>(LP, LH, nf, nn, T, w);
-                  nf = nn = 0;
-                  __syncwarp();
-                }
-              const int q = q0 + lane;
-              int L = 0;  // owner lane: number of lanes whose inclusive prefix is <= q
-#pragma unroll
-              for(int s = 16; s >= 1; s >>= 1)
-                {
-                  const int v = __shfl_sync(0xffffffffu, pinc, L + s - 1);
-                  if(v <= q)
-                    L += s;
-                }
-              L              = L < 31 ? L : 31;
-              const int ofp  = __shfl_sync(0xffffffffu, fp, L);
-              const int oexc = __shfl_sync(0xffffffffu, pexc, L);
-              bool keep      = false;
-              float4 pe      = make_float4(0, 0, 0, 0);
-              float ph = 0, pd2 = 0;
-              if(q < ptot)
-                {
-                  const int pi     = ofp + (q - oexc);
-                  const double4 pp = g_pm[pi];
-                  pe = make_float4((float)wrapd(pp.x - gx, w), (float)wrapd(pp.y - gy, w), (float)wrapd(pp.z - gz, w),
-                                   (float)pp.w);
-                  ph   = w.soft[g_pst[pi]];
-                  keep = pp.w != 0.0;
-                  const float dmx = fmaxf(fabsf(pe.x) - ex, 0.0f), dmy = fmaxf(fabsf(pe.y) - ey, 0.0f),
-                              dmz = fmaxf(fabsf(pe.z) - ez, 0.0f);
-                  pd2 = dmx * dmx + dmy * dmy + dmz * dmz;
-                  if(PERIODIC)
-                    keep = keep && pd2 < w.rcut2;
-                }
-              const float hn = fmaxf(h_grp, ph);
-              push(LP, LH, nf, nn, keep, pd2 < hn * hn, pe, ph, lt_mask);
-            }
           // node children of opened nodes -> stack (contiguous in breadth-first order)
           const int ncx  = (action == 2) ? nc : 0;
           const int cinc = wscan_incl(ncx, lane);
@@ -781,27 +859,14 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
           else if(lane == 0)
             atomicOr(err, 16);  // stack too small: the walk of this group is incomplete
           __syncwarp();
-          if(nf + nn >= kEvalAt)
-            {
-              WALK_STAT(0, nf + nn);
-              evaluate<PERIODIC, POT, TPL, EWALD>(LP, LH, nf, nn, T, w);
-              nf = nn = 0;
-              __syncwarp();
-            }
-        }
-      if(nf + nn > 0)
-        {
-          WALK_STAT(0, nf + nn);
-          evaluate<PERIODIC, POT, TPL, EWALD>(LP, LH, nf, nn, T, w);
-          __syncwarp();
         }
 #pragma unroll
       for(int k = 0; k < TPL; k++)
         {
-          const int s     = lane + 32 * k;
-          const int64_t t = t0 + s;
+          const int s = lane + 32 * k;
           if(s < cnt)
             {
+              const int64_t t    = tlist ? (int64_t)tlist[t0 + s] : t0 + s;
               acc_out[3 * t + 0] = T[k].dax;
               acc_out[3 * t + 1] = T[k].day;
               acc_out[3 * t + 2] = T[k].daz;
@@ -953,6 +1018,8 @@ void make_w32(const WalkConst &wc, W32Const *w)
   w->half_box  = wc.half_box;
   w->rcut      = (float)wc.rcut;
   w->rcut2     = (float)wc.rcut2;
+  // margin for the rounding of the FP32 separations and the box extents (relative ~1e-6)
+  w->rcut2_all = (float)(wc.rcut2 * (1.0 - 1.0 / 4096.0));
   w->asmthfac  = (float)wc.asmthfac;
   const double finv = wc.pm ? wc.asmthinv2 : 1.0;
   w->theta2    = (float)(wc.theta * wc.theta);
@@ -1086,6 +1153,7 @@ cudaError_t layout32_stage(gpugrav_ctx *c)
   GG_TRY(groups_stage(c));
   c->mark("l2 groups");
   c->layout32_valid = true;
+  c->groups_active  = false;
   return cudaSuccess;
 }
 
@@ -1142,7 +1210,8 @@ cudaError_t walk32_launch(gpugrav_ctx *c)
   kern<<<c->w32_blocks, 32 * kWarps, 0, st>>>(c->g_sm.as<double4>(), c->g_rel.as<float4>(), c->g_kids.as<int4>(),
                                               c->g_pm.as<double4>(), c->g_pst.as<uint8_t>(), c->s_pm.as<double4>(),
                                               c->s_st.as<uint8_t>(), c->oldacc_s.as<float>(), c->g_ngroups.as<int>(),
-                                              c->g_groups.as<int4>(), c->slice, c->nslices, (const W32Const *)c->scratch.p,
+                                              c->g_groups.as<int4>(), c->w_tlist, c->slice, c->nslices,
+                                              (const W32Const *)c->scratch.p,
                                               c->g_stack.as<int>(), work, c->acc_s.as<double>(), c->pot_s.as<double>(),
                                               c->nint_s.as<int32_t>(), (unsigned long long *)(c->counters.as<int>() + 32), err);
   return cudaGetLastError();
@@ -1170,9 +1239,9 @@ cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc)
 // measurement build only: read and reset the walk statistics of the current device
 extern "C" int gpugrav_walk_stats(unsigned long long *out)
 {
-  if(cudaMemcpyFromSymbol(out, gg::g_walk_stats, sizeof(unsigned long long) * 4) != cudaSuccess)
+  if(cudaMemcpyFromSymbol(out, gg::g_walk_stats, sizeof(unsigned long long) * 8) != cudaSuccess)
     return -1;
-  unsigned long long z[4] = {0, 0, 0, 0};
+  unsigned long long z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   return cudaMemcpyToSymbol(gg::g_walk_stats, z, sizeof(z)) == cudaSuccess ? 0 : -1;
 }
 #endif

@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(32 * kWarps, 12) k_walk64(const double4 *__res
                                                         const int2 *__restrict__ w_link, uint32_t n_entries,
                                                         const double4 *__restrict__ tpm, const uint8_t *__restrict__ tst,
                                                         const float *__restrict__ oldacc, int64_t t_begin, int64_t t_end,
-                                                        const WalkConst *__restrict__ wcp,
+                                                        const int32_t *__restrict__ tlist, const WalkConst *__restrict__ wcp,
                                                         double *__restrict__ acc_out, double *__restrict__ pot_out,
                                                         int32_t *__restrict__ nint_out, unsigned long long *__restrict__ total)
 {
@@ -64,8 +64,11 @@ __global__ void __launch_bounds__(32 * kWarps, 12) k_walk64(const double4 *__res
   __syncthreads();
 
   const int lane  = threadIdx.x & 31;
-  const int64_t tgt = t_begin + ((int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5)) * 32 + lane;
-  const bool valid  = tgt < t_end;
+  // position in the walk's target range; the target itself (sorted particle index) is the same
+  // position, or its entry in the list of active targets
+  const int64_t slot = t_begin + ((int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5)) * 32 + lane;
+  const bool valid   = slot < t_end;
+  const int64_t tgt  = valid && tlist ? (int64_t)tlist[slot] : slot;
 
   double pos_x = 0, pos_y = 0, pos_z = 0, aold = 0, h_i = 0;
   if(valid)
@@ -291,7 +294,8 @@ __global__ void __launch_bounds__(32 * kWarps, 12) k_walk64(const double4 *__res
 
 cudaError_t walk64_stage(gpugrav_ctx *c, const WalkConst &wc)
 {
-  const int64_t n       = c->n;
+  // targets: every particle, or the active list (gpugrav_walk_targets)
+  const int64_t n       = c->w_tlist ? c->w_ntargets : c->n;
   const int64_t t_begin = n * c->slice / c->nslices, t_end = n * (c->slice + 1) / c->nslices;
   const int64_t warps   = (t_end - t_begin + 31) / 32;
   const int64_t blocks  = warps > 0 ? (warps + kWarps - 1) / kWarps : 1;
@@ -299,7 +303,8 @@ cudaError_t walk64_stage(gpugrav_ctx *c, const WalkConst &wc)
                        : (wc.mns ? k_walk64<false, true> : k_walk64<false, false>);
   kern<<<(unsigned)blocks, 32 * kWarps, 0, c->stream>>>(
       c->w_sm.as<double4>(), c->w_cl.as<double4>(), c->w_link.as<int2>(), (uint32_t)c->n_entries, c->s_pm.as<double4>(),
-      c->s_st.as<uint8_t>(), c->oldacc_s.as<float>(), t_begin, t_end, c->wconst.as<WalkConst>(), c->acc_s.as<double>(), c->pot_s.as<double>(),
+      c->s_st.as<uint8_t>(), c->oldacc_s.as<float>(), t_begin, t_end, c->w_tlist, c->wconst.as<WalkConst>(),
+      c->acc_s.as<double>(), c->pot_s.as<double>(),
       c->nint_s.as<int32_t>(), (unsigned long long *)(c->counters.as<int>() + 32));
   return cudaGetLastError();
 }

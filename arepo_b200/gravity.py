@@ -142,6 +142,20 @@ class GravityTree:
         self._check(self.lib.gpugrav_walk(self._ctx, L.ptr(oldacc), L.ptr(acc), L.ptr(pot), L.ptr(ninter), mem))
         return acc, pot, ninter
 
+    def gravity_tree_targets(self, targets, oldacc=None, want_pot: bool = True):
+        """gravity_tree(timebin) for an active subset: `targets` are caller indices (TargetList,
+        src/gravity/gravtree.c:494-520); outputs (host arrays) in the order of `targets`."""
+        tg = np.ascontiguousarray(targets, np.int32)
+        nt = len(tg)
+        acc = np.empty((nt, 3), np.float64)
+        pot = np.empty(nt, np.float64) if want_pot else None
+        ninter = np.empty(nt, np.int32)
+        if oldacc is not None:
+            oldacc = np.ascontiguousarray(oldacc, np.float32)
+        self._check(self.lib.gpugrav_walk_targets(self._ctx, nt, L.ptr(tg), L.ptr(oldacc), L.ptr(acc), L.ptr(pot),
+                                                  L.ptr(ninter), L.MEM_HOST))
+        return acc, pot, ninter
+
     def compute_grav_accelerations(self, pos, mass, softtype, topnodes=None, pm_acc=None):
         """First-step sequence of compute_grav_accelerations (src/gravity/accel.c:58-80):
         Barnes-Hut pass, OldAcc = |a_tree + a_PM/G| (gravity_force_finalize, accel.c:237-255),

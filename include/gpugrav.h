@@ -188,7 +188,18 @@ int32_t gpugrav_build(gpugrav_ctx *ctx, const gpugrav_topnode *top, int32_t ntop
  * oldacc: n floats in caller order or NULL (zeros); acc: n*3 doubles; pot, ninter: n each or NULL.
  * All arrays in caller order, in memory of kind `mem`. */
 int32_t gpugrav_walk(gpugrav_ctx *ctx, const float *oldacc, double *acc, double *pot, int32_t *ninter, int32_t mem);
-/* Restrict the following walks (gpugrav_walk, gpugrav_compute) to slice `slice` of `nslices`
+/* The walk of an active subset: gravity_tree(timebin) builds TargetList from
+ * TimeBinsGravity.ActiveParticleList (src/gravity/gravtree.c:494-520) and walks only those particles
+ * while the tree holds all of them (the production caller under HIERARCHICAL_GRAVITY,
+ * src/time_integration/do_gravity_hydro.c:126-270).  targets: ntargets caller indices in [0, n), any
+ * order, each at most once (GPUGRAV_ERR_INVALID otherwise); the library walks them in Peano-Hilbert
+ * order.  oldacc: n floats in caller order (every particle's OldAcc, as for gpugrav_walk) or NULL;
+ * acc: ntargets*3, pot, ninter: ntargets each or NULL, in the order of `targets`.  FP64: per-target
+ * results bit-identical to gpugrav_walk's for the same particles; FP32: walk groups are formed from
+ * consecutive active targets.  Arrays (targets included) in memory of kind `mem`. */
+int32_t gpugrav_walk_targets(gpugrav_ctx *ctx, int64_t ntargets, const int32_t *targets, const float *oldacc, double *acc,
+                             double *pot, int32_t *ninter, int32_t mem);
+/* Restrict the following walks (gpugrav_walk, gpugrav_walk_targets, gpugrav_compute) to slice `slice` of `nslices`
  * contiguous slices of the targets in Peano-Hilbert order -- the reference's domain
  * decomposition into key segments (src/domain/domain_toplevel.c), applied to targets only: the
  * tree still holds every particle. FP32: slices are whole walk groups; FP64: target ranges.
