@@ -36,7 +36,7 @@ namespace
 #define GG_W32_EVAL_AT 192
 #endif
 #ifndef GG_W32_UNROLL
-#define GG_W32_UNROLL 4
+#define GG_W32_UNROLL 8
 #endif
 constexpr int kWarps   = GG_W32_WARPS;    // warps per block
 constexpr int kEvalAt  = GG_W32_EVAL_AT;  // evaluate once this many entries are queued

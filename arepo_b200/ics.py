@@ -99,6 +99,14 @@ def zeldovich_box(n1: int = 256, seed: int = 1003, pmgrid: int = 512, rms_cells:
     return d
 
 
+def zoom_box_softening(log2_half: int = 23, b: float = 0.02):
+    """Plummer-equivalent softening of the zoom box's two species: 1/40 of the mean spacing of the
+    uniform particles, and of the Plummer particles inside the half-mass radius 1.305 b."""
+    nh = 1 << log2_half
+    v_half = 4.0 / 3.0 * np.pi * (1.305 * b) ** 3
+    return ((1.0 / nh) ** (1.0 / 3.0) / 40.0, (v_half / (nh / 2)) ** (1.0 / 3.0) / 40.0)
+
+
 def zoom_box(log2_half: int = 23, seed: int = 1004, pmgrid: int = 512, b: float = 0.02, rtrunc: float = 0.1):
     """2^k low-resolution particles of mass 8m uniform in L=1 and 2^k high-resolution
     particles of mass m, Plummer (scale b) truncated at rtrunc around the box centre.
@@ -112,10 +120,7 @@ def zoom_box(log2_half: int = 23, seed: int = 1004, pmgrid: int = 512, b: float 
     pos = np.concatenate([lo, hi])
     mass = np.concatenate([np.full(nh, 8.0 * m), np.full(nh, m)])
     st = np.concatenate([np.zeros(nh, np.uint8), np.ones(nh, np.uint8)])
-    v_half = 4.0 / 3.0 * np.pi * (1.305 * b) ** 3  # Plummer half-mass radius 1.305 b
-    eps_lo = (1.0 / nh) ** (1.0 / 3.0) / 40.0
-    eps_hi = (v_half / (nh / 2)) ** (1.0 / 3.0) / 40.0
-    d = dict(pos=pos, mass=mass, softtype=st, softening=(eps_lo, eps_hi))
+    d = dict(pos=pos, mass=mass, softtype=st, softening=zoom_box_softening(log2_half, b))
     d.update(_treepm(pmgrid))
     return d
 

@@ -149,21 +149,22 @@ class ClockSampler:
 # --------------------------------------------------------------------------------------
 # CPU reference (oracle/_ref: the reference's own compiled code)
 # --------------------------------------------------------------------------------------
-CPU_SAMPLE_LOG2_HALF = 19   # N = 2^20 particles of the same zoom distribution
-CPU_SAMPLE_STRIDE = 64      # walk every 64th target, extrapolated to all
+CPU_LOG2_HALF = 23        # the GPU arm's zoom box: N = 2^24
+CPU_SAMPLE_STRIDE = 1024  # every 1024th target of the zoom box (16384 of 2^24) per timed walk
 
 
-def run_cpu_reference(procs: int, alpha: float, log2_half: int | None = None, stride: int | None = None):
-    """Reference step on the host: domain decomposition (keys, sort, top tree), construct_forcetree,
-    force_treeevaluate for a 1/stride sample of targets after a Barnes-Hut pass, by `procs` independent
-    processes that each walk a disjoint slice of the sample. Returns (particles/s, detail).
-    The sample defaults to CPU_SAMPLE_LOG2_HALF / CPU_SAMPLE_STRIDE, read at call time."""
+def run_cpu_reference(procs: int, alpha: float, reps: int, log2_half: int | None = None, stride: int | None = None):
+    """The reference's own code (oracle/_ref/ref_harness_pm, compiled from the reference sources) on the
+    same particles as the GPU arm: domain_Decomposition and construct_forcetree of every particle (timed
+    once), force_treeevaluate for every stride-th target in key order in a Barnes-Hut pass (OldAcc) and a
+    relative pass, then `reps` more timed walks of that sample by `procs` forked processes that share the
+    particles and the tree.  Each target's walk is independent, so the walk of all targets takes
+    (walk of the sample) x (targets / sample).  Returns a dict of the measured figures."""
     from arepo_b200 import ics
     from oracle import oracle as O
 
-    log2_half = CPU_SAMPLE_LOG2_HALF if log2_half is None else log2_half
     stride = CPU_SAMPLE_STRIDE if stride is None else stride
-
+    log2_half = CPU_LOG2_HALF if log2_half is None else log2_half
     exe = os.path.join(O.REF_DIR, "ref_harness_pm")
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
@@ -172,32 +173,43 @@ def run_cpu_reference(procs: int, alpha: float, log2_half: int | None = None, st
     import tempfile
 
     td = tempfile.mkdtemp()
-    fin = os.path.join(td, "in.bin")
+    fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
     O.write_input(fin, ic["pos"], ic["mass"], ic["softtype"])
-    eps = ic["softening"]
-    slice_len = (n + procs - 1) // procs
-    ps = []
-    for p in range(procs):
-        fout = os.path.join(td, f"out{p}.bin")
-        args = [exe, fin, fout, "box=1.0", f"asmth={ic['asmth']!r}", f"rcut={ic['rcut']!r}", "theta=0.7",
-                f"erracc={alpha!r}", f"eps0={eps[0]!r}", f"eps1={eps[1]!r}", "mdom=8", "tnf=2.5", "passes=2", "dump=0",
-                "gt=0", f"stride={stride}", f"first={p * slice_len}", f"count={min(slice_len, n - p * slice_len)}"]
-        ps.append((subprocess.Popen(args, stdout=subprocess.PIPE, stderr=subprocess.PIPE), fout))
-    times = []
-    for proc, fout in ps:
-        proc.communicate()
-        if proc.returncode != 0:
-            raise RuntimeError("reference harness failed")
-        r = O.read_output(fout)
-        times.append(r["time1"])  # relative pass: domain, build, walk(sample), -, targets, interactions
-    t = np.array(times)
-    domain, build = t[:, 0].max(), t[:, 1].max()
-    walk_full = (t[:, 2] * stride).max()  # each process walks its slice; extrapolate the 1/stride sample
-    step = domain + build + walk_full
-    ia = t[:, 5].sum() * stride
-    detail = {"n": n, "procs": procs, "domain_s": domain, "build_s": build, "walk_s_extrapolated": walk_full,
-              "interactions_per_particle": ia / n}
-    return n / step, detail
+    del ic
+    eps = ics.zoom_box_softening(log2_half)
+    a = ics.ASMTH / 512
+    args = [exe, fin, fout, "box=1.0", f"asmth={a!r}", f"rcut={ics.RCUT * a!r}", "theta=0.7", f"erracc={alpha!r}",
+            f"eps0={eps[0]!r}", f"eps1={eps[1]!r}", "mdom=8", "tnf=2.5", "passes=2", "dump=0", "gt=0", "lite=1",
+            f"stride={stride}", f"procs={procs}", f"reps={reps}"]
+    t0 = time.time()
+    r = subprocess.run(args, capture_output=True, text=True)
+    wall = time.time() - t0
+    for f in (fin, fout):
+        if os.path.exists(f):
+            os.remove(f)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference harness failed ({r.returncode}): {r.stderr[-500:]}")
+
+    def fields(line):
+        return {k: v for k, v in (w.split("=", 1) for w in line.replace("(", "").replace(")", "").replace(",", "").split()
+                                   if "=" in w)}
+
+    passes = [fields(l) for l in r.stdout.splitlines() if l.startswith("pass=")]
+    reps_ = [fields(l) for l in r.stdout.splitlines() if l.startswith("rep=")]
+    if len(passes) != 2 or len(reps_) != reps:
+        raise RuntimeError("unexpected reference harness output")
+    targets = int(reps_[0]["targets"])
+    return {"n": n, "targets": targets, "stride": stride, "procs": procs,
+            "domain_s": float(passes[0]["domain"]), "build_s": float(passes[1]["build"]),
+            "walk_s": [float(x["walk"]) for x in reps_],
+            "interactions_per_target": int(reps_[0]["interactions"]) / targets, "harness_wall_s": wall}
+
+
+def cpu_reference_value(d, walk_s):
+    """particles/s of one full step (domain decomposition + tree build + walk of every particle) from the
+    measured set-up and the walk of the sample, extrapolated linearly in the number of targets"""
+    step = d["domain_s"] + d["build_s"] + walk_s * d["n"] / d["targets"]
+    return d["n"] / step, step
 
 
 def cpu_info():
@@ -208,28 +220,36 @@ def cpu_info():
     return model, os.cpu_count()
 
 
+def cpu_sample_text(d, model):
+    return (f"reference C (oracle/_ref, the reference's own sources), {d['procs']} forked processes on {model}: the same "
+            f"N=2^{int(d['n']).bit_length() - 1} zoom box and ErrTolForceAcc; domain decomposition + tree build of all particles measured once "
+            f"({d['domain_s']:.1f} s + {d['build_s']:.1f} s); each step walks every {d['stride']}th target in key order "
+            f"({d['targets']} targets, {d['interactions_per_target']:.0f} interactions each); full-step particles/s "
+            f"= N / (set-up + sample walk x N/{d['targets']})")
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     model, ncpu = cpu_info()
-    procs = max(1, min(ncpu or 1, 16))
-    vals = []
-    for k in range(args.warmup + args.steps):
-        v, detail = run_cpu_reference(procs, args.err_tol_force_acc)
-        if k >= args.warmup:
-            vals.append(v)
+    procs = max(1, ncpu or 1)
+    d = run_cpu_reference(procs, args.err_tol_force_acc, args.warmup + args.steps)
+    timed = d["walk_s"][args.warmup:]
+    vals = [cpu_reference_value(d, w)[0] for w in timed]
     value = float(np.mean(vals))
+    ms = 1e3 * float(np.mean(timed))
+    detail = dict(d, walk_s=None, walk_s_timed=timed, full_step_s_extrapolated=cpu_reference_value(d, float(np.mean(timed)))[1])
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * detail["n"] / value, "higher_is_better": True, "scaling": "strong",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(workload_config(23, "fp64", args.err_tol_force_acc), cpu_sample=f"N=2^{CPU_SAMPLE_LOG2_HALF + 1} of the same zoom "
-                       f"distribution, 1/{CPU_SAMPLE_STRIDE} of targets walked and extrapolated"),
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded zoom box, arepo_b200/ics.py)",
+        "config": dict(workload_config(CPU_LOG2_HALF, "fp64", args.err_tol_force_acc),
+                       step="one timed step = the walk of the sample (every "
+                            f"{d['stride']}th target) by {procs} processes; value = full-step particles/s "
+                            "(measured domain decomposition and build + sample walk scaled to all targets)"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
-                         "sample": f"reference C (oracle/_ref), {procs} processes on {model}; N=2^{CPU_SAMPLE_LOG2_HALF + 1} "
-                                   f"zoom box, domain+build+walk, walk on 1/{CPU_SAMPLE_STRIDE} targets extrapolated",
-                         "detail": detail},
+                         "sample": cpu_sample_text(d, model), "detail": detail},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -715,11 +735,11 @@ def our_arm(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             model, ncpu = cpu_info()
-            v, detail = run_cpu_reference(1, args.err_tol_force_acc)
-            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
-                                    "sample": f"reference C (oracle/_ref) on 1 core of {model}: N=2^{CPU_SAMPLE_LOG2_HALF + 1} "
-                                              f"zoom box, domain+build+walk, walk on 1/{CPU_SAMPLE_STRIDE} targets extrapolated",
-                                    "detail": detail}
+            d = run_cpu_reference(max(1, ncpu or 1), args.err_tol_force_acc, 2, log2_half=lh)
+            v, step = cpu_reference_value(d, d["walk_s"][-1])
+            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": d["procs"], "kind": "reference",
+                                    "sample": cpu_sample_text(d, model),
+                                    "detail": dict(d, full_step_s_extrapolated=step)}
         except Exception as e:
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                                     "sample": f"unavailable: {e}"}

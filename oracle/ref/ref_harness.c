@@ -24,14 +24,22 @@
  *             passes (1 = BH only, 2 = BH then relative), dump (1 = write tree),
  *             stride (walk every stride-th particle in the timed loop), first, count
  *             (walk a contiguous slice of sorted targets; used for CPU timing),
- *             gt (1 = also run gravity_tree), tag (string printed with timings)
+ *             gt (1 = also run gravity_tree), tag (string printed with timings),
+ *             procs (walk the selected targets with that many forked processes, which share
+ *             the particles and the tree copy-on-write; targets dealt round-robin),
+ *             reps (after the last pass, walk the selected targets that many more times and
+ *             print each walk's wall time: the CPU timing of a bounded sample),
+ *             lite (1 = write only the timing sections, not the per-particle arrays)
  */
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/mman.h>
 #include <sys/time.h>
+#include <sys/wait.h>
+#include <unistd.h>
 
 #include "allvars.h"
 #include "proto.h"
@@ -87,30 +95,86 @@ static void split_key(peanokey k, uint64_t *hi, uint64_t *lo)
   *hi                 = (uint64_t)(u >> 64);
 }
 
-/* walk the selected sorted targets with the reference's per-target routine */
-static double walk_targets(int first, int count, int stride, double *acc, double *pot, int *ninter)
+/* one sorted target with the reference's per-target routine */
+static void walk_one(int i, double *acc, double *pot, int *ninter)
+{
+  gravdata_in in;
+  gravdata_out out;
+  for(int k = 0; k < 3; k++)
+    in.Pos[k] = P[i].Pos[k];
+  in.Type          = P[i].Type;
+  in.SofteningType = P[i].SofteningType;
+  in.OldAcc        = P[i].OldAcc;
+  in.Firstnode     = 0;
+  int n            = force_treeevaluate(&in, &out, i, 0, 0, 1, NULL, 0);
+  for(int k = 0; k < 3; k++)
+    acc[3 * i + k] = out.Acc[k];
+  pot[i]    = out.Potential;
+  ninter[i] = n;
+}
+
+/* walk the selected sorted targets; procs > 1: forked processes that share the particles and the
+ * tree copy-on-write, each walking every procs-th selected target, results in shared memory */
+static double walk_targets(int first, int count, int stride, int procs, double *acc, double *pot, int *ninter)
 {
   double t0 = wall();
-  for(int i = first; i < first + count; i += stride)
+  if(procs <= 1)
     {
-      gravdata_in in;
-      gravdata_out out;
-      for(int k = 0; k < 3; k++)
-        in.Pos[k] = P[i].Pos[k];
-      in.Type          = P[i].Type;
-      in.SofteningType = P[i].SofteningType;
-      in.OldAcc        = P[i].OldAcc;
-      in.Firstnode     = 0;
-      int n            = force_treeevaluate(&in, &out, i, 0, 0, 1, NULL, 0);
-      if(acc)
+      for(int i = first; i < first + count; i += stride)
+        walk_one(i, acc, pot, ninter);
+      return wall() - t0;
+    }
+  size_t n     = (size_t)NumPart;
+  size_t bytes = n * (3 * sizeof(double) + sizeof(double) + sizeof(int));
+  char *sh     = mmap(NULL, bytes, PROT_READ | PROT_WRITE, MAP_SHARED | MAP_ANONYMOUS, -1, 0);
+  if(sh == MAP_FAILED)
+    {
+      fprintf(stderr, "ref_harness: mmap of the shared results failed\n");
+      exit(3);
+    }
+  double *sacc = (double *)sh, *spot = sacc + 3 * n;
+  int *snint   = (int *)(spot + n);
+  fflush(stdout);
+  fflush(stderr);
+  pid_t *pids = malloc(sizeof(pid_t) * procs);
+  for(int c = 0; c < procs; c++)
+    {
+      pids[c] = fork();
+      if(pids[c] < 0)
         {
-          for(int k = 0; k < 3; k++)
-            acc[3 * i + k] = out.Acc[k];
-          pot[i]    = out.Potential;
-          ninter[i] = n;
+          fprintf(stderr, "ref_harness: fork failed\n");
+          exit(3);
+        }
+      if(pids[c] == 0)
+        {
+          for(long i = first + (long)stride * c; i < first + count; i += (long)stride * procs)
+            walk_one((int)i, sacc, spot, snint);
+          _exit(0);
         }
     }
-  return wall() - t0;
+  int bad = 0;
+  for(int c = 0; c < procs; c++)
+    {
+      int st = 0;
+      if(waitpid(pids[c], &st, 0) < 0 || !WIFEXITED(st) || WEXITSTATUS(st) != 0)
+        bad = 1;
+    }
+  double t = wall() - t0;
+  free(pids);
+  if(bad)
+    {
+      fprintf(stderr, "ref_harness: a walk process failed\n");
+      exit(3);
+    }
+  for(int i = first; i < first + count; i += stride)
+    {
+      for(int k = 0; k < 3; k++)
+        acc[3 * i + k] = sacc[3 * i + k];
+      pot[i]    = spot[i];
+      ninter[i] = snint[i];
+    }
+  munmap(sh, bytes);
+  return t;
 }
 
 static void dump_tree(FILE *f)
@@ -192,6 +256,11 @@ int main(int argc, char **argv)
   int first  = (int)arg_d(argc, argv, "first", 0);
   int count  = (int)arg_d(argc, argv, "count", n);
   int run_gt = (int)arg_d(argc, argv, "gt", 1);
+  int procs  = (int)arg_d(argc, argv, "procs", 1);
+  int reps   = (int)arg_d(argc, argv, "reps", 0);
+  int lite   = (int)arg_d(argc, argv, "lite", 0);
+  if(procs < 1)
+    procs = 1;
   if(first < 0 || first > n)
     first = 0;
   if(count < 0 || first + count > n)
@@ -306,14 +375,14 @@ int main(int argc, char **argv)
                     DomainCenter[2], DomainLen,       DomainInverseLen, DomainBigFac,   (double)NTopnodes};
   wr(fo, dom, 8, 10);
 
-  wsec(fo, "order", (int64_t)n * 8);
-  for(int i = 0; i < n; i++)
+  wsec(fo, "order", lite ? 0 : (int64_t)n * 8);
+  for(int i = 0; i < n && !lite; i++)
     {
       int64_t o = (int64_t)P[i].ID - 1;
       wr(fo, &o, 8, 1);
     }
-  wsec(fo, "keys", (int64_t)n * 16);
-  for(int i = 0; i < n; i++)
+  wsec(fo, "keys", lite ? 0 : (int64_t)n * 16);
+  for(int i = 0; i < n && !lite; i++)
     {
       peano1D xb = domain_double_to_int(((P[i].Pos[0] - DomainCorner[0]) * DomainInverseLen) + 1.0);
       peano1D yb = domain_double_to_int(((P[i].Pos[1] - DomainCorner[1]) * DomainInverseLen) + 1.0);
@@ -351,7 +420,7 @@ int main(int argc, char **argv)
       memset(acc, 0, sizeof(double) * 3 * n);
       memset(pot, 0, sizeof(double) * n);
       memset(ninter, 0, sizeof(int) * n);
-      double t_walk = walk_targets(first, count, stride, acc, pot, ninter);
+      double t_walk = walk_targets(first, count, stride, procs, acc, pot, ninter);
 
       double t_gt = 0;
       if(run_gt)
@@ -366,16 +435,29 @@ int main(int argc, char **argv)
       else if(All.TypeOfOpeningCriterion == 1)
         All.ErrTolTheta = 0; /* what gravity_tree() does at its end (gravity/gravtree.c:654-655) */
 
+      /* the bounded CPU timing: the same walk again, reps times, after the last pass's */
+      for(int r = 0; pass == passes - 1 && r < reps; r++)
+        {
+          double tr     = walk_targets(first, count, stride, procs, acc, pot, ninter);
+          long long nir = 0;
+          int ntr       = 0;
+          for(int i = first; i < first + count; i += stride)
+            nir += ninter[i], ntr++;
+          printf("rep=%d walk=%.6f targets=%d interactions=%lld procs=%d\n", r, tr, ntr, nir, procs);
+          fflush(stdout);
+        }
+
       char nm[16];
+      const size_t na = lite ? 0 : (size_t)n;
       snprintf(nm, sizeof(nm), "acc%d", pass);
-      wsec(fo, nm, (int64_t)n * 24);
-      wr(fo, acc, 8, 3 * (size_t)n);
+      wsec(fo, nm, (int64_t)na * 24);
+      wr(fo, acc, 8, 3 * na);
       snprintf(nm, sizeof(nm), "pot%d", pass);
-      wsec(fo, nm, (int64_t)n * 8);
-      wr(fo, pot, 8, n);
+      wsec(fo, nm, (int64_t)na * 8);
+      wr(fo, pot, 8, na);
       snprintf(nm, sizeof(nm), "ninter%d", pass);
-      wsec(fo, nm, (int64_t)n * 4);
-      wr(fo, ninter, 4, n);
+      wsec(fo, nm, (int64_t)na * 4);
+      wr(fo, ninter, 4, na);
       if(run_gt)
         {
           snprintf(nm, sizeof(nm), "gacc%d", pass);
@@ -394,8 +476,8 @@ int main(int argc, char **argv)
       free_tree();
 
       snprintf(nm, sizeof(nm), "oldacc%d", pass);
-      wsec(fo, nm, (int64_t)n * 4);
-      for(int i = 0; i < n; i++)
+      wsec(fo, nm, (int64_t)na * 4);
+      for(int i = 0; i < (int)na; i++)
         {
           float oa = P[i].OldAcc;
           wr(fo, &oa, 4, 1);

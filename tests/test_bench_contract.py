@@ -20,7 +20,7 @@ def small_bench(monkeypatch):
         pytest.skip("reference harness not built (needs the reference sources)")
     import bench
 
-    monkeypatch.setattr(bench, "CPU_SAMPLE_LOG2_HALF", 11)  # N = 4096
+    monkeypatch.setattr(bench, "CPU_LOG2_HALF", 11)  # N = 4096
     monkeypatch.setattr(bench, "CPU_SAMPLE_STRIDE", 8)
     return bench
 
@@ -37,10 +37,11 @@ def test_reference_arm_json_line(small_bench, monkeypatch, capsys):
     assert line["steps"] == 1 and line["n_gpus"] == 1
     cb = line["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == line["value"]
-    assert "N=2^12" in cb["sample"]
+    assert "N=2^12" in cb["sample"] and cb["cores"] == cb["detail"]["procs"]
+    assert line["ms_per_step"] == pytest.approx(1e3 * cb["detail"]["walk_s_timed"][0])
     e2e = line["e2e"]
     assert e2e["value"] == line["value"] and e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
-    assert line["config"]["workload"].startswith("zoom box N=2^24")
+    assert line["config"]["workload"].startswith("zoom box N=2^12")
 
 
 def test_reference_arm_other_ranks_print_nothing(small_bench, monkeypatch, capsys):
