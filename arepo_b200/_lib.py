@@ -37,7 +37,11 @@ MEM_HOST = 0
 MEM_DEVICE = 1
 PREC_FP64 = 0
 PREC_FP32 = 1
+PREC_FP64_GROUP = 2  # the FP32 walk's algorithm in FP64 arithmetic (precision ablation)
 FLAG_MULTIPLE_NODE_SOFTENING = 1
+FLAG_MINIMUM_OPENING_ANGLE = 2
+FLAG_ALLOW_DIRECT_SUMMATION = 4
+DIRECT_SUMMATION_THRESHOLD = 3000
 DIRECT_FULL = 0
 DIRECT_CUT = 1
 
@@ -166,6 +170,7 @@ _SIGS = {
     "gpugrav_build": (C.c_int32, [_P, _P, C.c_int32]),
     "gpugrav_walk": (C.c_int32, [_P, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_walk_targets": (C.c_int32, [_P, C.c_int64, _P, _P, _P, _P, _P, C.c_int32]),
+    "gpugrav_gravity_direct": (C.c_int32, [_P, C.c_int64, _P, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_set_target_slice": (C.c_int32, [_P, C.c_int32, C.c_int32]),
     "gpugrav_pm_periodic": (C.c_int32, [_P, C.c_int32, C.c_int64, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_set_ewald_table": (C.c_int32, [_P, C.c_int32, _P, _P, _P, _P]),
@@ -239,6 +244,7 @@ def make_params(
     multiple_domains: int = 8,
     precision: int = PREC_FP64,
     multiple_node_softening: bool = False,
+    minimum_opening_angle: bool = False,
 ) -> Params:
     """softening: Plummer-equivalent epsilon per softening type. The spline support is
     ForceSoftening = 2.8 * epsilon with a trailing zero entry (set_softenings,
@@ -260,7 +266,8 @@ def make_params(
     p.top_node_factor = top_node_factor
     p.multiple_domains = multiple_domains
     p.precision = precision
-    p.flags = FLAG_MULTIPLE_NODE_SOFTENING if multiple_node_softening else 0
+    p.flags = (FLAG_MULTIPLE_NODE_SOFTENING if multiple_node_softening else 0) | \
+        (FLAG_MINIMUM_OPENING_ANGLE if minimum_opening_angle else 0)
     return p
 
 

@@ -170,7 +170,151 @@ __global__ void k_map_targets(const int64_t *__restrict__ tg, int64_t nt, const 
   if(t < nt)
     out[t] = inv[tg[t]];
 }
+// gravity_direct (src/gravity/gravdirect.c:61-257) with force_evaluate_direct's pair arithmetic
+// (src/gravity/forcetree_walk.c:557-708): the n particles are targets and sources; every thread sums
+// all sources in their order with the reference's operations (FP64, no contraction), so the result is
+// bit-identical.  Flag bit 1: a softening type >= nsofttypes.
+__global__ void __launch_bounds__(kTile) k_gravity_direct(const double *__restrict__ pos, const double *__restrict__ mass,
+                                                          const uint8_t *__restrict__ st, int64_t n,
+                                                          const WalkConst *__restrict__ wcp, double *__restrict__ acc,
+                                                          double *__restrict__ pot, int *__restrict__ flag)
+{
+  __shared__ double4 src[kTile];
+  __shared__ double hsrc[kTile];
+  const WalkConst &w = *wcp;
+  const int64_t i    = (int64_t)blockIdx.x * kTile + threadIdx.x;
+  double pos_x = 0, pos_y = 0, pos_z = 0, h_i = 0;
+  if(i < n)
+    {
+      pos_x = pos[3 * i + 0];
+      pos_y = pos[3 * i + 1];
+      pos_z = pos[3 * i + 2];
+      if(st[i] >= w.nsoft)
+        atomicOr(flag, 1);
+      h_i = w.soft[st[i] < w.nsoft ? st[i] : 0];
+    }
+  double acc_x = 0, acc_y = 0, acc_z = 0, pt = 0;
+  for(int64_t jb = 0; jb < n && n > 1; jb += kTile)
+    {
+      __syncthreads();
+      const int64_t j = jb + threadIdx.x;
+      if(j < n)
+        {
+          src[threadIdx.x]  = make_double4(pos[3 * j + 0], pos[3 * j + 1], pos[3 * j + 2], mass[j]);
+          hsrc[threadIdx.x] = w.soft[st[j] < w.nsoft ? st[j] : 0];
+        }
+      __syncthreads();
+      const int cnt = (int)((n - jb) < kTile ? (n - jb) : kTile);
+      if(i < n)
+        for(int q = 0; q < cnt; q++)
+          {
+            const double4 s  = src[q];
+            const double h_j = hsrc[q];
+            double hmax      = (h_j > h_i) ? h_j : h_i;
+            double dx = s.x - pos_x, dy = s.y - pos_y, dz = s.z - pos_z;
+            if(w.periodic)
+              {
+                dx = (dx > w.half_box) ? (dx - w.box) : ((dx < -w.half_box) ? (dx + w.box) : dx);
+                dy = (dy > w.half_box) ? (dy - w.box) : ((dy < -w.half_box) ? (dy + w.box) : dy);
+                dz = (dz > w.half_box) ? (dz - w.box) : ((dz < -w.half_box) ? (dz + w.box) : dz);
+              }
+            double r2 = dx * dx + dy * dy + dz * dz;
+            double m  = s.w;
+            double r  = sqrt(r2);
+            double factor_force = 0, factor_pot = 0;
+            if(w.pm)
+              {
+                double tabentry = w.asmthfac * r;
+                int tabindex    = (int)tabentry;
+                if(tabindex >= kNtab)
+                  continue;
+                double tabweight = tabentry - tabindex;
+                factor_force     = (1.0 - tabweight) * w.tab_force[tabindex] + tabweight * w.tab_force[tabindex + 1];
+                factor_pot       = (1.0 - tabweight) * w.tab_pot[tabindex] + tabweight * w.tab_pot[tabindex + 1];
+              }
+            double fac, wp;
+            if(r >= hmax)
+              {
+                double rinv  = 1.0 / r;
+                double rinv3 = rinv * rinv * rinv;
+                if(w.pm)
+                  {
+                    fac = rinv3 + rinv * factor_force * w.asmthinv2;
+                    wp  = rinv * factor_pot;
+                  }
+                else
+                  {
+                    fac = rinv3;
+                    wp  = -rinv;
+                  }
+              }
+            else
+              {
+                double h_inv  = 1.0 / hmax;
+                double h3_inv = h_inv * h_inv * h_inv;
+                double u      = r * h_inv;
+                if(u < 0.5)
+                  {
+                    double u2 = u * u;
+                    fac       = h3_inv * (SF1 + u2 * (SF2 * u + SF3));
+                    wp        = h_inv * (SF4 + u2 * (SF5 + u2 * (SF6 * u + SF7)));
+                  }
+                else
+                  {
+                    double u2 = u * u;
+                    double u3 = u2 * u;
+                    fac       = h3_inv * (SF8 + SF9 * u + SF10 * u2 + SF11 * u3 + SF12 / u3);
+                    wp        = h_inv * (SF13 + SF14 / u + u2 * (SF1 + u * (SF15 + u * (SF16 + SF17 * u))));
+                  }
+                if(w.pm && r > 0)
+                  {
+                    double rinv = 1.0 / r;
+                    fac += rinv * factor_force * w.asmthinv2;
+                    wp += rinv * (factor_pot + 1.0);
+                  }
+              }
+            pt += m * wp;
+            fac *= m;
+            acc_x += dx * fac;
+            acc_y += dy * fac;
+            acc_z += dz * fac;
+            if(w.ewald)
+              {
+                double fcorr[3], pcorr;
+                ewald_corr(dx, dy, dz, w, fcorr, pcorr);
+                acc_x += m * fcorr[0];
+                acc_y += m * fcorr[1];
+                acc_z += m * fcorr[2];
+                pt += m * pcorr;
+              }
+          }
+    }
+  if(i < n)
+    {
+      acc[3 * i + 0] = acc_x;
+      acc[3 * i + 1] = acc_y;
+      acc[3 * i + 2] = acc_z;
+      if(pot)
+        pot[i] = pt;
+    }
+}
+
+__global__ void k_fill_i32(int32_t *__restrict__ a, int64_t n, int32_t v)
+{
+  for(int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = v;
+}
 }  // namespace
+
+cudaError_t gravity_direct_stage(gpugrav_ctx *c, int64_t n, const double *d_pos, const double *d_mass, const uint8_t *d_st,
+                                 double *d_acc, double *d_pot, int32_t *d_nint, int *d_flag)
+{
+  k_gravity_direct<<<(unsigned)((n + kTile - 1) / kTile), kTile, 0, c->stream>>>(d_pos, d_mass, d_st, n, c->wconst.as<WalkConst>(),
+                                                                                   d_acc, d_pot, d_flag);
+  if(d_nint)
+    k_fill_i32<<<(unsigned)((n + 255) / 256 < 2368 ? (n + 255) / 256 : 2368), 256, 0, c->stream>>>(d_nint, n, (int32_t)n);
+  return cudaGetLastError();
+}
 
 cudaError_t direct_stage(gpugrav_ctx *c, const WalkConst &wc, int64_t nt, const int64_t *d_targets, int cut, double *d_acc,
                          double *d_pot)

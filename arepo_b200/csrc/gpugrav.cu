@@ -196,11 +196,12 @@ int gg::validate_params(const gpugrav_params *p)
     }
   if(!(p->err_tol_theta >= 0) || !(p->err_tol_force_acc >= 0))
     return GPUGRAV_ERR_INVALID;
-  if(p->precision != GPUGRAV_PREC_FP64 && p->precision != GPUGRAV_PREC_FP32)
+  if(p->precision != GPUGRAV_PREC_FP64 && p->precision != GPUGRAV_PREC_FP32 && p->precision != GPUGRAV_PREC_FP64_GROUP)
     return GPUGRAV_ERR_INVALID;
   if(p->multiple_domains < 1 || p->multiple_domains > 512 || !(p->top_node_factor > 0))
     return GPUGRAV_ERR_INVALID;
-  if((p->flags & ~GPUGRAV_FLAG_MULTIPLE_NODE_SOFTENING) != 0 || p->reserved != 0)
+  if((p->flags & ~(GPUGRAV_FLAG_MULTIPLE_NODE_SOFTENING | GPUGRAV_FLAG_MINIMUM_OPENING_ANGLE | GPUGRAV_FLAG_ALLOW_DIRECT_SUMMATION)) != 0 ||
+     p->reserved != 0)
     return GPUGRAV_ERR_INVALID;
   return GPUGRAV_OK;
 }
@@ -211,6 +212,7 @@ void gg::make_walk_const(const gpugrav_params &p, WalkConst *w)
   memset(w, 0, sizeof(*w));
   w->periodic = p.periodic;
   w->mns      = (p.flags & GPUGRAV_FLAG_MULTIPLE_NODE_SOFTENING) ? 1 : 0;
+  w->minangle = (p.flags & GPUGRAV_FLAG_MINIMUM_OPENING_ANGLE) ? 1 : 0;
   w->nsoft    = p.nsofttypes;
   w->pm       = p.periodic && p.asmth > 0;
   w->ewald    = p.periodic && !(p.asmth > 0);
@@ -667,8 +669,8 @@ int walk_impl(gpugrav_ctx *c, int64_t nt, const int32_t *targets, const float *o
     }
   k_gather_f32<<<grid_for(n, 256), 256, 0, st>>>(old_dev, c->perm.as<uint32_t>(), n, c->oldacc_s.as<float>());
   // active list: sorted positions in key order (targets_stage checks range and duplicates)
-  const bool fp32 = c->prm.precision == GPUGRAV_PREC_FP32;
-  const int cap   = 32 * ((c->walk32_tpl == 1 || c->multi || wc.ewald) ? 1 : 2);  // FP32 group size
+  const bool fp32 = c->prm.precision != GPUGRAV_PREC_FP64;  // the group walk (FP32, or its FP64 form)
+  const int cap   = 32 * gg::walk32_tpl(c);                    // group size
   int64_t a = 0, b = nout;  // this call's target slice of the active list
   c->w_tlist    = nullptr;
   c->w_ntargets = 0;
@@ -782,6 +784,69 @@ int walk_impl(gpugrav_ctx *c, int64_t nt, const int32_t *targets, const float *o
   c->timings.walk_kernel_launches = 1;
   return GPUGRAV_OK;
 }
+
+// gravity_direct for n particles (targets = sources), outputs in the given order
+int gravity_direct_impl(gpugrav_ctx *c, int64_t n, const double *pos, const double *mass, const uint8_t *softtype, double *acc,
+                        double *pot, int32_t *ninter, int32_t mem)
+{
+  if(!c)
+    return GPUGRAV_ERR_INVALID;
+  if(n < 1 || n >= (int64_t)1 << 30 || !pos || !mass || !softtype || !acc || (mem != GPUGRAV_MEM_HOST && mem != GPUGRAV_MEM_DEVICE))
+    return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_gravity_direct: need n >= 1 and pos, mass, softtype, acc");
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->stream;
+  c->loaded = c->built = false;  // the particle buffers are reused
+  WalkConst wc;
+  make_walk_const(c->prm, &wc);
+  if(wc.ewald)
+    {
+      CK(gg::ewald_ensure(c), "Ewald tables");
+      wc.ewd = c->ewd.as<double>();
+    }
+  CK(cudaMemcpyAsync(c->wconst.p, &wc, sizeof(wc), cudaMemcpyHostToDevice, st), "walk constants");
+  const double *d_pos = pos, *d_mass = mass;
+  const uint8_t *d_st = softtype;
+  double *d_acc = acc, *d_pot = pot;
+  int32_t *d_nint = ninter;
+  if(mem == GPUGRAV_MEM_HOST)
+    {
+      if(c->pos_in.ensure(n * 24) != cudaSuccess || c->mass_in.ensure(n * 8) != cudaSuccess || c->st_in.ensure(n + 16) != cudaSuccess ||
+         c->out_acc.ensure(n * 24) != cudaSuccess || c->out_pot.ensure(n * 8) != cudaSuccess ||
+         c->out_nint.ensure(n * 4) != cudaSuccess)
+        return fail(c, GPUGRAV_ERR_OOM, "gpugrav_gravity_direct: device allocation");
+      CK(cudaMemcpyAsync(c->pos_in.p, pos, n * 24, cudaMemcpyHostToDevice, st), "upload positions");
+      CK(cudaMemcpyAsync(c->mass_in.p, mass, n * 8, cudaMemcpyHostToDevice, st), "upload masses");
+      CK(cudaMemcpyAsync(c->st_in.p, softtype, n, cudaMemcpyHostToDevice, st), "upload softening types");
+      d_pos  = c->pos_in.as<double>();
+      d_mass = c->mass_in.as<double>();
+      d_st   = c->st_in.as<uint8_t>();
+      d_acc  = c->out_acc.as<double>();
+      d_pot  = pot ? c->out_pot.as<double>() : nullptr;
+      d_nint = ninter ? c->out_nint.as<int32_t>() : nullptr;
+    }
+  int *flag = c->counters.as<int>() + 17;
+  CK(cudaMemsetAsync(flag, 0, sizeof(int), st), "reset flag");
+  cudaEventRecord(c->ev[8], st);
+  CK(gg::gravity_direct_stage(c, n, d_pos, d_mass, d_st, d_acc, d_pot, d_nint, flag), "direct summation");
+  cudaEventRecord(c->ev[9], st);
+  if(mem == GPUGRAV_MEM_HOST)
+    {
+      CK(cudaMemcpyAsync(acc, d_acc, n * 24, cudaMemcpyDeviceToHost, st), "download acc");
+      if(pot)
+        CK(cudaMemcpyAsync(pot, d_pot, n * 8, cudaMemcpyDeviceToHost, st), "download pot");
+      if(ninter)
+        CK(cudaMemcpyAsync(ninter, d_nint, n * 4, cudaMemcpyDeviceToHost, st), "download interactions");
+    }
+  int bad = 0;
+  CK(cudaMemcpyAsync(&bad, flag, sizeof(int), cudaMemcpyDeviceToHost, st), "flags");
+  CK(cudaStreamSynchronize(st), "direct summation");
+  if(bad)
+    return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_gravity_direct: softening type >= nsofttypes");
+  c->timings.walk_ms              = elapsed(c->ev[8], c->ev[9]);
+  c->timings.interactions         = n * n;
+  c->timings.walk_kernel_launches = 1;
+  return GPUGRAV_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -800,10 +865,18 @@ int32_t gpugrav_walk_targets(gpugrav_ctx *c, int64_t ntargets, const int32_t *ta
   return walk_impl(c, ntargets, targets ? targets : &none, oldacc, acc, pot, ninter, mem);
 }
 
+int32_t gpugrav_gravity_direct(gpugrav_ctx *c, int64_t n, const double *pos, const double *mass, const uint8_t *softtype,
+                               double *acc, double *pot, int32_t mem)
+{
+  return gravity_direct_impl(c, n, pos, mass, softtype, acc, pot, nullptr, mem);
+}
+
 int32_t gpugrav_compute(gpugrav_ctx *c, int64_t n, const double *pos, const double *mass, const uint8_t *softtype,
                         const float *oldacc, const gpugrav_domain *dom, const gpugrav_topnode *top, int32_t ntop, double *acc,
                         double *pot, int32_t *ninter, int32_t mem)
 {
+  if(c && (c->prm.flags & GPUGRAV_FLAG_ALLOW_DIRECT_SUMMATION) && n < GPUGRAV_DIRECT_SUMMATION_THRESHOLD)
+    return gravity_direct_impl(c, n, pos, mass, softtype, acc, pot, ninter, mem);  // gravity(), accel.c:103-110
   int s = gpugrav_load(c, n, pos, mass, softtype, mem, dom);
   if(s != GPUGRAV_OK)
     return s;

@@ -61,7 +61,7 @@ struct WalkConst
   int32_t ewald;     // pure periodic tree: Ewald correction per interaction (periodic without PM)
   int32_t mns;       // MULTIPLE_NODE_SOFTENING: nodes used per softening type
   int32_t nsoft;
-  int32_t pad0;
+  int32_t minangle;  // ACTIVATE_MINIMUM_OPENING_ANGLE: minimum opening angle in the relative criterion
   const double *w_mpt;  // FP64 walk: per-type masses of each walk entry (nodes), nsoft each
   double ewd_fac_intp;       // 2 EN / L
   const double *ewd;         // device tables fx | fy | fz | pot, (EN+1)^3 each
@@ -277,7 +277,16 @@ cudaError_t node_arrays(gpugrav_ctx *c, int64_t nn);
 cudaError_t layout32_stage(gpugrav_ctx *c);
 cudaError_t direct_stage(gpugrav_ctx *c, const WalkConst &wc, int64_t nt, const int64_t *d_targets, int cut, double *d_acc,
                          double *d_pot);
+cudaError_t gravity_direct_stage(gpugrav_ctx *c, int64_t n, const double *d_pos, const double *d_mass, const uint8_t *d_st,
+                                 double *d_acc, double *d_pot, int32_t *d_nint, int *d_flag);
 void make_walk_const(const gpugrav_params &p, WalkConst *wc);
+// targets per lane of the group walk: 2 only on request (GPUGRAV_WALK32_TPL) for the FP32 TreePM or
+// isolated walk of one system
+inline int walk32_tpl(const gpugrav_ctx *c)
+{
+  const bool ewald = c->prm.periodic && !(c->prm.asmth > 0);
+  return (c->walk32_tpl == 1 || c->multi || ewald || c->prm.precision != GPUGRAV_PREC_FP32) ? 1 : 2;
+}
 // GPUGRAV_OK or GPUGRAV_ERR_INVALID: ABI version, softening table (finite, >= 0, zero end entry),
 // box size, TreePM split (asmth, rcut, rcut_cells > 0 unless asmth == 0), tolerances, flags
 int validate_params(const gpugrav_params *p);

@@ -44,13 +44,11 @@ constexpr int kUnroll  = GG_W32_UNROLL;   // list entries in flight per lane in 
 #ifndef GG_W32_MINBLOCKS
 #define GG_W32_MINBLOCKS 5  // blocks per SM the register budget is sized for (96 registers a thread)
 #endif
-// capacity: accepted nodes (<= 32) join a list holding fewer than kEvalAt entries; particles are
-// added at most 32 per round and the list is evaluated first whenever a round could overflow it.
-// Entries inside some target's softening length go to a separate, smaller near list, evaluated as
-// soon as it holds kNearAt entries.
-constexpr int kListCap = kEvalAt + 64;
-constexpr int kNearAt  = 64;
-constexpr int kNearCap = kNearAt + 64;
+// capacity (Cap below): accepted nodes (<= 32) join a list holding fewer than kEvalAt entries;
+// particles are added at most 32 per round and the list is evaluated first whenever a round could
+// overflow it.  Entries inside some target's softening length go to a separate, smaller near list,
+// evaluated as soon as it holds kNearAt entries.
+constexpr int kNearAt = 64;
 constexpr int kStackCap = 16384;  // traversal stack entries per warp (global memory)
 // A node that the group-box test opens although it is smaller than 1/kVote of the box's largest side
 // and nearer to the box than that is tested against every target of the group instead (opened
@@ -60,23 +58,64 @@ constexpr int kStackCap = 16384;  // traversal stack entries per warp (global me
 // core down to single particles.
 constexpr float kVote = 16.0f;
 
-#define SF1 10.666666666667f
-#define SF2 32.0f
-#define SF3 (-38.4f)
-#define SF4 (-2.8f)
-#define SF5 5.333333333333f
-#define SF6 6.4f
-#define SF7 (-9.6f)
-#define SF8 21.333333333333f
-#define SF9 (-48.0f)
-#define SF10 38.4f
-#define SF11 (-10.666666666667f)
-#define SF12 (-0.066666666667f)
-#define SF13 (-3.2f)
-#define SF14 0.066666666667f
-#define SF15 (-16.0f)
-#define SF16 9.6f
-#define SF17 (-2.133333333333f)
+// cubic-spline softening coefficients (src/main/allvars.h:557-573), rounded to the walk's type
+#define SF1 10.666666666667
+#define SF2 32.0
+#define SF3 (-38.4)
+#define SF4 (-2.8)
+#define SF5 5.333333333333
+#define SF6 6.4
+#define SF7 (-9.6)
+#define SF8 21.333333333333
+#define SF9 (-48.0)
+#define SF10 38.4
+#define SF11 (-10.666666666667)
+#define SF12 (-0.066666666667)
+#define SF13 (-3.2)
+#define SF14 0.066666666667
+#define SF15 (-16.0)
+#define SF16 9.6
+#define SF17 (-2.133333333333)
+
+// The arithmetic type R of the evaluation: float (the fast form) or double (the same group walk in
+// FP64, the precision ablation of the fast form).  List capacities per type: double entries take
+// twice the shared memory.
+template <typename R>
+struct Cap
+{
+  static constexpr int eval     = sizeof(R) == 4 ? kEvalAt : 96;
+  static constexpr int list     = eval + 64;
+  static constexpr int near_at  = sizeof(R) == 4 ? kNearAt : 32;
+  static constexpr int near_cap = near_at + 64;
+};
+template <typename R>
+struct V4T;
+template <>
+struct V4T<float>
+{
+  typedef float4 type;
+};
+template <>
+struct V4T<double>
+{
+  typedef double4 type;
+};
+template <typename R>
+using V4 = typename V4T<R>::type;
+template <typename R>
+__device__ __forceinline__ V4<R> mk4(double x, double y, double z, double m)
+{
+  V4<R> v;
+  v.x = (R)x;
+  v.y = (R)y;
+  v.z = (R)z;
+  v.w = (R)m;
+  return v;
+}
+__device__ __forceinline__ float fmaR(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fmaR(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float maxR(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double maxR(double a, double b) { return fmax(a, b); }
 
 struct W32Const
 {
@@ -87,12 +126,14 @@ struct W32Const
   int periodic, bh;
   float soft[GPUGRAV_MAX_SOFTTYPES + 1];
   float4 tab[kNtab + 1];  // (f[i], f[i+1] - f[i], p[i], p[i+1] - p[i]): force table times 1/Asmth^2, potential table
+  double rcut2_d, asmthfac_d;  // FP64 walk: Rcut^2 and the table index factor in double
+  double4 tab64[kNtab + 1];    // FP64 walk: the table above in double
   const float4 *ewd;       // Ewald correction (fx, fy, fz, pot) per table entry (pure periodic tree)
   float ewd_fac;           // 2 EN / L
   int mns;                 // MULTIPLE_NODE_SOFTENING: nodes used per softening type
   const float *mpt;        // per-type node masses, breadth-first order, nsoft each
   int nsoft;
-  int pad2;
+  int minangle;            // ACTIVATE_MINIMUM_OPENING_ANGLE
 };
 
 // ------------------------------------------------------------------------------
@@ -222,6 +263,11 @@ __device__ __forceinline__ float rsqrt_normal(float x)
   return y;
 }
 
+__device__ __forceinline__ float rsqrtR(float x) { return rsqrt_normal(x); }
+__device__ __forceinline__ double rsqrtR(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rcut2_of(const W32Const &w, float) { return w.rcut2; }
+__device__ __forceinline__ double rcut2_of(const W32Const &w, double) { return w.rcut2_d; }
+
 // Short-range factors of the TreePM split at separation r: linear interpolation of the force
 // (scaled by 1/Asmth^2) and potential tables between nodes floor(te) and floor(te) + 1,
 // te = r * asmthfac, as the reference does (src/gravity/forcetree_walk.c:366-379).  Adding 1.5 * 2^23 with rounding toward minus
@@ -238,12 +284,26 @@ __device__ __forceinline__ void short_range(float r, const W32Const &w, float &f
   ff              = fmaf(tw, t.y, t.x);
   fpt             = fmaf(tw, t.w, t.z);
 }
+// the same in double: floor(te) by conversion
+template <bool CLAMP = true>
+__device__ __forceinline__ void short_range(double r, const W32Const &w, double &ff, double &fpt)
+{
+  const double te = r * w.asmthfac_d;
+  int i           = (int)te;
+  if(CLAMP)
+    i = min(i, kNtab - 1);
+  const double tw = te - i;
+  const double4 t = w.tab64[i];
+  ff              = fma(tw, t.y, t.x);
+  fpt             = fma(tw, t.w, t.z);
+}
 
 // Per-target state of a lane (targets per lane: TPL).
+template <typename R>
 struct Tgt
 {
-  float x, y, z, h;         // position relative to the group centre, softening
-  float ax, ay, az, pot;    // FP32 partial sums of the current list batch
+  R x, y, z, h;             // position relative to the group centre, softening
+  R ax, ay, az, pot;        // partial sums of the current list batch
   double dax, day, daz, dpot;  // batch partials accumulated in FP64
   int ni;
 };
@@ -277,19 +337,20 @@ __device__ __forceinline__ float4 ewald_corr32(float dx, float dy, float dz, con
 // separation (the target itself) gives a huge 1/r but r = 0 (CLAMP); it lies inside the softening
 // length unless that is zero, where the reference's kernel has no finite value either.  far() and
 // near() both call this, so they agree on which side of the softening length every pair lies.
+template <typename R>
 struct Sep
 {
-  float dx, dy, dz, r2, rinv, r;
+  R dx, dy, dz, r2, rinv, r;
 };
-template <bool CLAMP = true>
-__device__ __forceinline__ Sep separation(const float4 e, const Tgt &T)
+template <typename R, bool CLAMP = true>
+__device__ __forceinline__ Sep<R> separation(const V4<R> e, const Tgt<R> &T)
 {
-  Sep s;
+  Sep<R> s;
   s.dx   = e.x - T.x;
   s.dy   = e.y - T.y;
   s.dz   = e.z - T.z;
-  s.r2   = fmaf(s.dx, s.dx, fmaf(s.dy, s.dy, s.dz * s.dz));
-  s.rinv = rsqrt_normal(CLAMP ? fmaxf(s.r2, 1.0e-30f) : s.r2);
+  s.r2   = fmaR(s.dx, s.dx, fmaR(s.dy, s.dy, s.dz * s.dz));
+  s.rinv = rsqrtR(CLAMP ? maxR(s.r2, (R)(sizeof(R) == 4 ? 1.0e-30 : 1.0e-60)) : s.r2);
   s.r    = s.r2 * s.rinv;
   return s;
 }
@@ -303,39 +364,39 @@ __device__ __forceinline__ Sep separation(const float4 e, const Tgt &T)
 // and reported by the return value, and near() adds the spline kernel for it.  Without CHECK the list
 // entry is known to lie outside the softening length of every target of the group.  The Ewald
 // correction (EWALD: pure periodic tree, nearest image) is taken here for every pair.
-template <bool PERIODIC, bool POT, bool EWALD = false, bool CHECK = true, bool MASK = true>
-__device__ __forceinline__ bool far(const float4 e, const float hj, Tgt &T, const W32Const &w)
+template <typename R, bool PERIODIC, bool POT, bool EWALD = false, bool CHECK = true, bool MASK = true>
+__device__ __forceinline__ bool far(const V4<R> e, const R hj, Tgt<R> &T, const W32Const &w)
 {
   constexpr bool PAIRWISE = MASK || CHECK;  // Rcut mask and count per pair
   // outside every target's softening length (no CHECK) r > 0 unless the softening is zero
-  const Sep s = separation<CHECK>(e, T);
-  bool in     = true;
-  float ff = 0.0f, fpt = 0.0f;
+  const Sep<R> s = separation<R, CHECK>(e, T);
+  bool in        = true;
+  R ff = 0, fpt = 0;
   if(PERIODIC)
     {
       if(PAIRWISE)
-        in = s.r2 < w.rcut2;
+        in = s.r2 < rcut2_of(w, R(0));
       short_range<PAIRWISE>(s.r, w, ff, fpt);
     }
   // force m (1/r^3 + f_s / (r Asmth^2)) = (m/r) (1/r^2 + f_s'), potential (m/r) p_s (Newtonian: -m/r);
   // 1/r^2 stays finite at the clamped r = 0, so masking m/r masks both
-  const bool soft = CHECK && s.r < fmaxf(T.h, hj);
-  const float m   = in ? e.w : 0.0f;
-  const float mr  = soft ? 0.0f : m * s.rinv;
-  const float fm  = mr * (PERIODIC ? fmaf(s.rinv, s.rinv, ff) : s.rinv * s.rinv);
-  T.ax            = fmaf(s.dx, fm, T.ax);
-  T.ay            = fmaf(s.dy, fm, T.ay);
-  T.az            = fmaf(s.dz, fm, T.az);
+  const bool soft = CHECK && s.r < maxR(T.h, hj);
+  const R m       = in ? e.w : R(0);
+  const R mr      = soft ? R(0) : m * s.rinv;
+  const R fm      = mr * (PERIODIC ? fmaR(s.rinv, s.rinv, ff) : s.rinv * s.rinv);
+  T.ax            = fmaR(s.dx, fm, T.ax);
+  T.ay            = fmaR(s.dy, fm, T.ay);
+  T.az            = fmaR(s.dz, fm, T.az);
   if(POT)
-    T.pot = PERIODIC ? fmaf(mr, fpt, T.pot) : T.pot - mr;
+    T.pot = PERIODIC ? fmaR(mr, fpt, T.pot) : T.pot - mr;
   if(EWALD)
     {
-      const float4 c = ewald_corr32(s.dx, s.dy, s.dz, w);
-      T.ax           = fmaf(m, c.x, T.ax);
-      T.ay           = fmaf(m, c.y, T.ay);
-      T.az           = fmaf(m, c.z, T.az);
+      const float4 c = ewald_corr32((float)s.dx, (float)s.dy, (float)s.dz, w);
+      T.ax           = fmaR(m, (R)c.x, T.ax);
+      T.ay           = fmaR(m, (R)c.y, T.ay);
+      T.az           = fmaR(m, (R)c.z, T.az);
       if(POT)
-        T.pot = fmaf(m, c.w, T.pot);
+        T.pot = fmaR(m, (R)c.w, T.pot);
     }
   if(PAIRWISE)
     T.ni += in ? 1 : 0;  // list entries all have mass != 0
@@ -345,51 +406,51 @@ __device__ __forceinline__ bool far(const float4 e, const float hj, Tgt &T, cons
 // The softened kernel of one target against one list entry, for a pair inside the softening length
 // (nothing otherwise): the reference's spline (src/gravity/forcetree_walk.c:421-455), plus the
 // TreePM short-range correction of the Newtonian part away from r = 0.
-template <bool PERIODIC, bool POT>
-__device__ __forceinline__ void near(const float4 e, const float hj, Tgt &T, const W32Const &w)
+template <typename R, bool PERIODIC, bool POT>
+__device__ __forceinline__ void near(const V4<R> e, const R hj, Tgt<R> &T, const W32Const &w)
 {
-  const Sep s      = separation(e, T);
-  const float hmax = fmaxf(T.h, hj);
+  const Sep<R> s = separation<R>(e, T);
+  const R hmax   = maxR(T.h, hj);
   if(!(s.r < hmax))
     return;
-  const float h_inv  = 1.0f / hmax;
-  const float h3_inv = h_inv * h_inv * h_inv;
-  const float u      = s.r * h_inv;
-  const float u2     = u * u;
-  float fac, wp = 0.0f;
-  if(u < 0.5f)
+  const R h_inv  = R(1) / hmax;
+  const R h3_inv = h_inv * h_inv * h_inv;
+  const R u      = s.r * h_inv;
+  const R u2     = u * u;
+  R fac, wp = 0;
+  if(u < R(0.5))
     {
-      fac = h3_inv * fmaf(u2, fmaf(SF2, u, SF3), SF1);
+      fac = h3_inv * fmaR(u2, fmaR((R)SF2, u, (R)SF3), (R)SF1);
       if(POT)
-        wp = h_inv * fmaf(u2, fmaf(u2, fmaf(SF6, u, SF7), SF5), SF4);
+        wp = h_inv * fmaR(u2, fmaR(u2, fmaR((R)SF6, u, (R)SF7), (R)SF5), (R)SF4);
     }
   else
     {
-      const float u3 = u2 * u;
-      fac = h3_inv * (SF8 + SF9 * u + SF10 * u2 + SF11 * u3 + SF12 / u3);
+      const R u3 = u2 * u;
+      fac = h3_inv * ((R)SF8 + (R)SF9 * u + (R)SF10 * u2 + (R)SF11 * u3 + (R)SF12 / u3);
       if(POT)
-        wp = h_inv * (SF13 + SF14 / u + u2 * (SF1 + u * (SF15 + u * (SF16 + SF17 * u))));
+        wp = h_inv * ((R)SF13 + (R)SF14 / u + u2 * ((R)SF1 + u * ((R)SF15 + u * ((R)SF16 + (R)SF17 * u))));
     }
   bool in = true;
   if(PERIODIC)
     {
-      in = s.r2 < w.rcut2;
-      if(s.r > 0.0f)
+      in = s.r2 < rcut2_of(w, R(0));
+      if(s.r > R(0))
         {
-          float ff, fpt;
+          R ff, fpt;
           short_range(s.r, w, ff, fpt);
-          fac = fmaf(s.rinv, ff, fac);
+          fac = fmaR(s.rinv, ff, fac);
           if(POT)
-            wp = fmaf(s.rinv, fpt + 1.0f, wp);
+            wp = fmaR(s.rinv, fpt + R(1), wp);
         }
     }
-  const float m  = in ? e.w : 0.0f;
-  const float fm = fac * m;
-  T.ax           = fmaf(s.dx, fm, T.ax);
-  T.ay           = fmaf(s.dy, fm, T.ay);
-  T.az           = fmaf(s.dz, fm, T.az);
+  const R m  = in ? e.w : R(0);
+  const R fm = fac * m;
+  T.ax       = fmaR(s.dx, fm, T.ax);
+  T.ay       = fmaR(s.dy, fm, T.ay);
+  T.az       = fmaR(s.dz, fm, T.az);
   if(POT)
-    T.pot = fmaf(m, wp, T.pot);
+    T.pot = fmaR(m, wp, T.pot);
 }
 
 #ifdef GG_WALK32_STATS
@@ -418,48 +479,48 @@ namespace
 // them), in blocks of kUnroll entries evaluated without branches.  CHECK (near list): a block in
 // which some pair lies inside the softening length (the targets' own particles, close neighbours)
 // is revisited for those pairs.  MASK: per-pair Rcut mask and count (see far()).
-template <bool PERIODIC, bool POT, int TPL, bool EWALD, bool CHECK, bool MASK>
-__device__ __forceinline__ void evaluate_region(const float4 *__restrict__ LP, const float *__restrict__ LH, int nl, Tgt (&T)[TPL],
+template <typename R, bool PERIODIC, bool POT, int TPL, bool EWALD, bool CHECK, bool MASK>
+__device__ __forceinline__ void evaluate_region(const V4<R> *__restrict__ LP, const R *__restrict__ LH, int nl, Tgt<R> (&T)[TPL],
                                                 const W32Const &w)
 {
   int j = 0;
   for(; j + kUnroll <= nl; j += kUnroll)
     {
-      float4 e[kUnroll];
-      float hj[kUnroll];
+      V4<R> e[kUnroll];
+      R hj[kUnroll];
 #pragma unroll
       for(int u = 0; u < kUnroll; u++)
         {
           e[u]  = LP[j + u];
-          hj[u] = CHECK ? LH[j + u] : 0.0f;
+          hj[u] = CHECK ? LH[j + u] : R(0);
         }
       bool soft = false;
 #pragma unroll
       for(int u = 0; u < kUnroll; u++)
 #pragma unroll
         for(int k = 0; k < TPL; k++)
-          soft |= far<PERIODIC, POT, EWALD, CHECK, MASK>(e[u], hj[u], T[k], w);
+          soft |= far<R, PERIODIC, POT, EWALD, CHECK, MASK>(e[u], hj[u], T[k], w);
       if(CHECK && soft)
         {
 #pragma unroll 1
           for(int u = 0; u < kUnroll; u++)
             {
-              const float4 eu = LP[j + u];
-              const float hu  = LH[j + u];
+              const V4<R> eu = LP[j + u];
+              const R hu     = LH[j + u];
 #pragma unroll
               for(int k = 0; k < TPL; k++)
-                near<PERIODIC, POT>(eu, hu, T[k], w);
+                near<R, PERIODIC, POT>(eu, hu, T[k], w);
             }
         }
     }
   for(; j < nl; j++)
     {
-      const float4 e = LP[j];
-      const float hj = CHECK ? LH[j] : 0.0f;
+      const V4<R> e = LP[j];
+      const R hj    = CHECK ? LH[j] : R(0);
 #pragma unroll
       for(int k = 0; k < TPL; k++)
-        if(far<PERIODIC, POT, EWALD, CHECK, MASK>(e, hj, T[k], w) && CHECK)
-          near<PERIODIC, POT>(e, hj, T[k], w);
+        if(far<R, PERIODIC, POT, EWALD, CHECK, MASK>(e, hj, T[k], w) && CHECK)
+          near<R, PERIODIC, POT>(e, hj, T[k], w);
     }
 }
 
@@ -467,23 +528,24 @@ __device__ __forceinline__ void evaluate_region(const float4 *__restrict__ LP, c
 // every target of the group, those inside Rcut of every target at the bottom (growing up, `na`),
 // the others at the top (growing down, `nb`).  Near buffer (`nn`): entries inside some target's
 // softening length, with their softening lengths.
+template <typename R>
 struct List
 {
-  float4 *P;
-  float4 *NP;
-  float *NH;
+  V4<R> *P;
+  V4<R> *NP;
+  R *NH;
   int na, nb, nn;
 };
 
 // Evaluates and empties the list, then folds the batch partials into the FP64 sums.
-template <bool PERIODIC, bool POT, int TPL, bool EWALD = false>
-__device__ __forceinline__ void evaluate(List &L, Tgt (&T)[TPL], const W32Const &w)
+template <typename R, bool PERIODIC, bool POT, int TPL, bool EWALD = false>
+__device__ __forceinline__ void evaluate(List<R> &L, Tgt<R> (&T)[TPL], const W32Const &w)
 {
   WALK_STAT(4, L.na);
   WALK_STAT(5, L.nb);
-  evaluate_region<PERIODIC, POT, TPL, EWALD, false, false>(L.P, nullptr, L.na, T, w);
-  evaluate_region<PERIODIC, POT, TPL, EWALD, false, true>(L.P + kListCap - L.nb, nullptr, L.nb, T, w);
-  evaluate_region<PERIODIC, POT, TPL, EWALD, true, true>(L.NP, L.NH, L.nn, T, w);
+  evaluate_region<R, PERIODIC, POT, TPL, EWALD, false, false>(L.P, nullptr, L.na, T, w);
+  evaluate_region<R, PERIODIC, POT, TPL, EWALD, false, true>(L.P + Cap<R>::list - L.nb, nullptr, L.nb, T, w);
+  evaluate_region<R, PERIODIC, POT, TPL, EWALD, true, true>(L.NP, L.NH, L.nn, T, w);
 #pragma unroll
   for(int k = 0; k < TPL; k++)
     {
@@ -492,21 +554,25 @@ __device__ __forceinline__ void evaluate(List &L, Tgt (&T)[TPL], const W32Const 
       T[k].day += T[k].ay;
       T[k].daz += T[k].az;
       T[k].dpot += T[k].pot;
-      T[k].ax = T[k].ay = T[k].az = T[k].pot = 0.0f;
+      T[k].ax = T[k].ay = T[k].az = T[k].pot = R(0);
     }
   L.na = L.nb = L.nn = 0;
 }
 
 // true when a push round of up to 32 entries could overflow a buffer
-__device__ __forceinline__ bool list_full(const List &L) { return L.na + L.nb + 32 > kListCap || L.nn + 32 > kNearCap; }
+template <typename R>
+__device__ __forceinline__ bool list_full(const List<R> &L)
+{
+  return L.na + L.nb + 32 > Cap<R>::list || L.nn + 32 > Cap<R>::near_cap;
+}
 
 // Appends one entry per lane that keeps one to the warp's list.  The entry (x, y, z relative to the
 // group centre, mass) lies at squared distance d2 from the nearest point of the group box (half
 // extents bx, by, bz); hn is the larger of the group's largest softening (with margin) and the
 // entry's own.  Closer than hn: near list.  Otherwise, when its farthest distance from the box is
 // below Rcut (with margin) or there is no Rcut: inside Rcut of every target; else the border region.
-template <bool PERIODIC>
-__device__ __forceinline__ void push(List &L, bool keep, const float4 e, float h, float d2, float hn, float bx, float by, float bz,
+template <typename R, bool PERIODIC>
+__device__ __forceinline__ void push(List<R> &L, bool keep, const V4<R> e, R h, float d2, float hn, float bx, float by, float bz,
                                      const W32Const &w, unsigned lt_mask)
 {
   int cls = 2;
@@ -515,7 +581,7 @@ __device__ __forceinline__ void push(List &L, bool keep, const float4 e, float h
       cls = 0;
       if(PERIODIC)
         {
-          const float fx = fabsf(e.x) + bx, fy = fabsf(e.y) + by, fz = fabsf(e.z) + bz;
+          const float fx = fabsf((float)e.x) + bx, fy = fabsf((float)e.y) + by, fz = fabsf((float)e.z) + bz;
           cls = (fmaf(fx, fx, fmaf(fy, fy, fz * fz)) < w.rcut2_all) ? 0 : 1;
         }
     }
@@ -526,7 +592,7 @@ __device__ __forceinline__ void push(List &L, bool keep, const float4 e, float h
       if(cls == 0)
         L.P[L.na + __popc(ka & lt_mask)] = e;
       else if(cls == 1)
-        L.P[kListCap - 1 - (L.nb + __popc(kb & lt_mask))] = e;
+        L.P[Cap<R>::list - 1 - (L.nb + __popc(kb & lt_mask))] = e;
       else
         {
           const int q = L.nn + __popc(kn & lt_mask);
@@ -539,8 +605,8 @@ __device__ __forceinline__ void push(List &L, bool keep, const float4 e, float h
   L.nn += __popc(kn);
 }
 
-template <bool PERIODIC, bool POT, int TPL, bool EWALD = false>
-__global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const double4 *__restrict__ g_sm, const float4 *__restrict__ g_rel,
+template <bool PERIODIC, bool POT, int TPL, bool EWALD = false, typename R = float>
+__global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS : 3) k_walk32(const double4 *__restrict__ g_sm, const float4 *__restrict__ g_rel,
                                                         const int4 *__restrict__ g_kids, const double4 *__restrict__ g_pm,
                                                         const uint8_t *__restrict__ g_pst, const double4 *__restrict__ tpm,
                                                         const uint8_t *__restrict__ tst, const float *__restrict__ oldacc,
@@ -553,9 +619,9 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                                                         int *__restrict__ err)
 {
   __shared__ W32Const w;
-  __shared__ float4 il_p[kWarps][kListCap];
-  __shared__ float4 il_np[kWarps][kNearCap];
-  __shared__ float il_nh[kWarps][kNearCap];
+  __shared__ V4<R> il_p[kWarps][Cap<R>::list];
+  __shared__ V4<R> il_np[kWarps][Cap<R>::near_cap];
+  __shared__ R il_nh[kWarps][Cap<R>::near_cap];
   for(int t = threadIdx.x; t < (int)(sizeof(W32Const) / 4); t += blockDim.x)
     ((int *)&w)[t] = ((const int *)wcp)[t];
   __syncthreads();
@@ -564,7 +630,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
   const int lane         = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
   int *stack             = stack_base + ((int64_t)blockIdx.x * kWarps + warp) * kStackCap;
-  List L;
+  List<R> L;
   L.P  = il_p[warp];
   L.NP = il_np[warp];
   L.NH = il_nh[warp];
@@ -621,14 +687,14 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
       // box side squared over kVote^2: a node smaller than this and closer than it gets the per-target vote
       const float side     = 2.0f * fmaxf(ex, fmaxf(ey, ez));
       const float vote_r2  = side * side * (1.0f / (kVote * kVote));
-      Tgt T[TPL];
+      Tgt<R> T[TPL];
 #pragma unroll
       for(int k = 0; k < TPL; k++)
         {
-          T[k].x = (float)(p[k].x - gx), T[k].y = (float)(p[k].y - gy), T[k].z = (float)(p[k].z - gz);
+          T[k].x = (R)(p[k].x - gx), T[k].y = (R)(p[k].y - gy), T[k].z = (R)(p[k].z - gz);
           const int sk = lane + 32 * k < cnt ? lane + 32 * k : 0;
-          T[k].h       = w.soft[tst[tlist ? (int64_t)tlist[t0 + sk] : t0 + sk]];
-          T[k].ax = T[k].ay = T[k].az = T[k].pot = 0.0f;
+          T[k].h       = (R)w.soft[tst[tlist ? (int64_t)tlist[t0 + sk] : t0 + sk]];
+          T[k].ax = T[k].ay = T[k].az = T[k].pot = R(0);
           T[k].dax = T[k].day = T[k].daz = T[k].dpot = 0.0;
           T[k].ni = 0;
         }
@@ -649,17 +715,18 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
       // per-lane state of the last node step, read by the pending items
       int node = -1, action = 0, fp = 0, pinc = 0, pexc = 0;
       bool split = false;
-      float4 entry = make_float4(0, 0, 0, 0);
+      V4<R> entry  = mk4<R>(0, 0, 0, 0);
       float ent_d2 = 0.0f;  // squared distance of the entry from the group box
       while(true)
         {
           const int queued = L.na + L.nb + L.nn;
           const bool flush = (t_next < t_end || q0 < ptot) ? list_full(L)
-                                                           : (sp > 0 ? (queued >= kEvalAt || L.nn >= kNearAt) : queued > 0);
+                                                           : (sp > 0 ? (queued >= Cap<R>::eval || L.nn >= Cap<R>::near_at)
+                                                                     : queued > 0);
           if(flush)
             {
               WALK_STAT(0, queued);
-              evaluate<PERIODIC, POT, TPL, EWALD>(L, T, w);
+              evaluate<R, PERIODIC, POT, TPL, EWALD>(L, T, w);
               __syncwarp();
             }
           if(t_next < t_end)
@@ -669,8 +736,8 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
               // this equals the single entry, the kernel being linear in the mass
               const int t    = t_next++;
               const float mt = (action == 1 && split) ? w.mpt[(int64_t)node * w.nsoft + t] : 0.0f;
-              push<PERIODIC>(L, mt != 0.0f, make_float4(entry.x, entry.y, entry.z, mt), w.soft[t], ent_d2,
-                             fmaxf(h_grp, w.soft[t]), ex, ey, ez, w, lt_mask);
+              push<R, PERIODIC>(L, mt != 0.0f, mk4<R>(entry.x, entry.y, entry.z, mt), (R)w.soft[t], ent_d2,
+                                fmaxf(h_grp, w.soft[t]), ex, ey, ez, w, lt_mask);
               continue;
             }
           if(q0 < ptot)
@@ -691,23 +758,22 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
               const int ofp  = __shfl_sync(0xffffffffu, fp, owner);
               const int oexc = __shfl_sync(0xffffffffu, pexc, owner);
               bool keep      = false;
-              float4 pe      = make_float4(0, 0, 0, 0);
+              V4<R> pe       = mk4<R>(0, 0, 0, 0);
               float ph = 0, pd2 = 0;
               if(q < ptot)
                 {
                   const int pi     = ofp + (q - oexc);
                   const double4 pp = g_pm[pi];
-                  pe = make_float4((float)wrapd(pp.x - gx, w), (float)wrapd(pp.y - gy, w), (float)wrapd(pp.z - gz, w),
-                                   (float)pp.w);
+                  pe   = mk4<R>(wrapd(pp.x - gx, w), wrapd(pp.y - gy, w), wrapd(pp.z - gz, w), pp.w);
                   ph   = w.soft[g_pst[pi]];
                   keep = pp.w != 0.0;
-                  const float dmx = fmaxf(fabsf(pe.x) - ex, 0.0f), dmy = fmaxf(fabsf(pe.y) - ey, 0.0f),
-                              dmz = fmaxf(fabsf(pe.z) - ez, 0.0f);
+                  const float dmx = fmaxf(fabsf((float)pe.x) - ex, 0.0f), dmy = fmaxf(fabsf((float)pe.y) - ey, 0.0f),
+                              dmz = fmaxf(fabsf((float)pe.z) - ez, 0.0f);
                   pd2 = dmx * dmx + dmy * dmy + dmz * dmz;
                   if(PERIODIC)
                     keep = keep && pd2 < w.rcut2;
                 }
-              push<PERIODIC>(L, keep, pe, ph, pd2, fmaxf(h_grp, ph), ex, ey, ez, w, lt_mask);
+              push<R, PERIODIC>(L, keep, pe, (R)ph, pd2, fmaxf(h_grp, ph), ex, ey, ez, w, lt_mask);
               continue;
             }
           if(sp == 0)
@@ -724,7 +790,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
           __syncwarp();
 
           action = 0;  // 1 accept, 2 open
-          entry  = make_float4(0, 0, 0, 0);
+          entry  = mk4<R>(0, 0, 0, 0);
           ent_d2 = 0.0f;
           split  = false;  // MULTIPLE_NODE_SOFTENING: accepted node listed per type
           float hj = 0;
@@ -740,7 +806,8 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
               const int4 kd    = g_kids[node];
               if(sm.w != 0.0)
                 {
-                  const float sx = (float)wrapd(sm.x - gx, w), sy = (float)wrapd(sm.y - gy, w), sz = (float)wrapd(sm.z - gz, w);
+                  const double dsx = wrapd(sm.x - gx, w), dsy = wrapd(sm.y - gy, w), dsz = wrapd(sm.z - gz, w);
+                  const float sx = (float)dsx, sy = (float)dsy, sz = (float)dsz;
                   const float cx = sx + rel.x, cy = sy + rel.y, cz = sz + rel.z;
                   const float L  = rel.w;
                   const float m  = (float)sm.w;
@@ -761,7 +828,10 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                       if(bh)
                         open = L2 > rmin2 * w.theta2;
                       else
-                        open = (L2 > rmin2 * 1.44f) || (m * L2 > rmin2 * rmin2 * aold_min) ||
+                        // with ACTIVATE_MINIMUM_OPENING_ANGLE the mass test also needs the node to span more than
+                        // 0.4 radian from the nearest point of the box (conservative for every target)
+                        open = (L2 > rmin2 * 1.44f) ||
+                               (m * L2 > rmin2 * rmin2 * aold_min && (!w.minangle || L2 > rmin2 * 0.16f)) ||
                                (fabsf(cx) < 0.6f * L + ex && fabsf(cy) < 0.6f * L + ey && fabsf(cz) < 0.6f * L + ez);
                       if(!open && hj > h_min)
                         {
@@ -784,7 +854,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                               vote      = true;
                               vote_keep = !PERIODIC || rmin2 < w.rcut2;
                               vrel      = rel;
-                              entry     = make_float4(sx, sy, sz, m);
+                              entry     = mk4<R>(dsx, dsy, dsz, sm.w);
                               ent_d2    = rmin2;
                             }
                         }
@@ -792,7 +862,7 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                         {
                           // accepted; a node whose CoM is beyond Rcut of every target contributes nothing
                           action = 1;
-                          entry  = make_float4(sx, sy, sz, m);
+                          entry  = mk4<R>(dsx, dsy, dsz, sm.w);
                           ent_d2 = rmin2;
                         }
                     }
@@ -807,20 +877,21 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
               for(int k = 0; k < TPL; k++)
                 for(int i = 0; i < 32; i++)
                   {
-                    const float tx = __shfl_sync(0xffffffffu, T[k].x, i), ty = __shfl_sync(0xffffffffu, T[k].y, i),
-                                tz = __shfl_sync(0xffffffffu, T[k].z, i), th = __shfl_sync(0xffffffffu, T[k].h, i),
+                    const float tx = (float)__shfl_sync(0xffffffffu, T[k].x, i), ty = (float)__shfl_sync(0xffffffffu, T[k].y, i),
+                                tz = (float)__shfl_sync(0xffffffffu, T[k].z, i), th = (float)__shfl_sync(0xffffffffu, T[k].h, i),
                                 ta = __shfl_sync(0xffffffffu, a_l[k], i);
                     if(vote && !need && i + 32 * k < cnt)
                       {
-                        const float dx = entry.x - tx, dy = entry.y - ty, dz = entry.z - tz;
+                        const float enx = (float)entry.x, eny = (float)entry.y, enz = (float)entry.z;
+                        const float dx = enx - tx, dy = eny - ty, dz = enz - tz;
                         const float r2 = dx * dx + dy * dy + dz * dz;
                         bool o;
                         if(bh)
                           o = L2 > r2 * w.theta2;
                         else
-                          o = (L2 > r2 * 1.44f) || (entry.w * L2 > r2 * r2 * ta) ||
-                              (fabsf(entry.x + vrel.x - tx) < 0.6f * L && fabsf(entry.y + vrel.y - ty) < 0.6f * L &&
-                               fabsf(entry.z + vrel.z - tz) < 0.6f * L);
+                          o = (L2 > r2 * 1.44f) || ((float)entry.w * L2 > r2 * r2 * ta && (!w.minangle || L2 > r2 * 0.16f)) ||
+                              (fabsf(enx + vrel.x - tx) < 0.6f * L && fabsf(eny + vrel.y - ty) < 0.6f * L &&
+                               fabsf(enz + vrel.z - tz) < 0.6f * L);
                         if(!o && !w.mns && hj > th && r2 < hj * hj)
                           o = true;
                         need = o;
@@ -833,9 +904,9 @@ __global__ void __launch_bounds__(32 * kWarps, GG_W32_MINBLOCKS) k_walk32(const 
                   nc = np = 0;
                 }
             }
-          // accepted nodes -> list (the list holds fewer than kEvalAt entries, so 32 more fit);
+          // accepted nodes -> list (the list holds fewer than Cap::eval entries, so 32 more fit);
           // nodes used per softening type follow as pending items
-          push<PERIODIC>(L, action == 1 && !split, entry, hj, ent_d2, fmaxf(h_grp, hj), ex, ey, ez, w, lt_mask);
+          push<R, PERIODIC>(L, action == 1 && !split, entry, (R)hj, ent_d2, fmaxf(h_grp, hj), ex, ey, ez, w, lt_mask);
           t_next = 0;
           t_end  = __ballot_sync(0xffffffffu, action == 1 && split) ? w.nsoft : 0;
           // particles of opened nodes: pending rounds
@@ -1028,6 +1099,7 @@ void make_w32(const WalkConst &wc, W32Const *w)
   w->bh        = wc.bh;
   w->ewd_fac   = (float)wc.ewd_fac_intp;
   w->mns       = wc.mns;
+  w->minangle  = wc.minangle;
   w->nsoft     = wc.nsoft;
   for(int i = 0; i <= GPUGRAV_MAX_SOFTTYPES; i++)
     w->soft[i] = (float)wc.soft[i];
@@ -1036,7 +1108,13 @@ void make_w32(const WalkConst &wc, W32Const *w)
       float f0 = (float)(finv * wc.tab_force[i]), f1 = (float)(finv * ((i < kNtab) ? wc.tab_force[i + 1] : wc.tab_force[i]));
       float p0 = wc.tab_pot[i], p1 = (i < kNtab) ? wc.tab_pot[i + 1] : wc.tab_pot[i];
       w->tab[i] = make_float4(f0, f1 - f0, p0, p1 - p0);
+      // FP64 walk: the reference's float table entries, scaled and differenced in double
+      const double d0 = finv * wc.tab_force[i], d1 = finv * ((i < kNtab) ? wc.tab_force[i + 1] : wc.tab_force[i]);
+      const double q0 = wc.tab_pot[i], q1 = (i < kNtab) ? wc.tab_pot[i + 1] : wc.tab_pot[i];
+      w->tab64[i]     = make_double4(d0, d1 - d0, q0, q1 - q0);
     }
+  w->rcut2_d    = wc.rcut2;
+  w->asmthfac_d = wc.asmthfac;
 }
 }  // namespace
 
@@ -1085,7 +1163,7 @@ cudaError_t groups_stage(gpugrav_ctx *c)
   const int64_t n = c->n;
   cudaStream_t st = c->stream;
   const bool ewald = c->prm.periodic && !(c->prm.asmth > 0);  // the Ewald variant walks one target per lane
-  const int cap    = 32 * ((c->walk32_tpl == 1 || c->multi || ewald) ? 1 : 2);
+  const int cap    = 32 * walk32_tpl(c);
   GG_TRY(cudaMemsetAsync(c->g_ngroups.p, 0, sizeof(int), st));
   if(n == 0)
     return cudaSuccess;
@@ -1183,8 +1261,14 @@ cudaError_t walk32_prepare(gpugrav_ctx *c, const WalkConst &wc)
   GG_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const bool periodic = wc.pm != 0;  // TreePM split (Rcut, erfc table)
   const bool pot      = c->want_pot;
-  const int tpl       = (c->walk32_tpl == 1 || c->multi || wc.ewald) ? 1 : 2;
-  Walk32Kernel kern = wc.ewald ? (pot ? k_walk32<false, true, 1, true> : k_walk32<false, false, 1, true>)
+  const int tpl       = walk32_tpl(c);
+  // the group walk in FP64 arithmetic (precision ablation): TreePM and isolated, one target per lane
+  const bool fp64     = c->prm.precision == GPUGRAV_PREC_FP64_GROUP;
+  if(fp64 && wc.ewald)
+    return cudaErrorNotSupported;
+  Walk32Kernel kern = fp64 ? (periodic ? (pot ? k_walk32<true, true, 1, false, double> : k_walk32<true, false, 1, false, double>)
+                                       : (pot ? k_walk32<false, true, 1, false, double> : k_walk32<false, false, 1, false, double>))
+                    : wc.ewald ? (pot ? k_walk32<false, true, 1, true> : k_walk32<false, false, 1, true>)
                       : tpl == 2 ? (periodic ? (pot ? k_walk32<true, true, 2> : k_walk32<true, false, 2>)
                                              : (pot ? k_walk32<false, true, 2> : k_walk32<false, false, 2>))
                                  : (periodic ? (pot ? k_walk32<true, true, 1> : k_walk32<true, false, 1>)

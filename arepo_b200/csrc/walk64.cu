@@ -158,7 +158,8 @@ __global__ void __launch_bounds__(32 * kWarps, 12) k_walk64(const double4 *__res
                   next = i + 1;
                   continue;
                 }
-              if(mass * len2 > r2 * r2 * aold)
+              // ACTIVATE_MINIMUM_OPENING_ANGLE adds a minimum angle to the mass test (forcetree_walk.c:266-271)
+              if(mass * len2 > r2 * r2 * aold && (!w.minangle || len2 > r2 * (0.4 * 0.4)))
                 {
                   next = i + 1;
                   continue;

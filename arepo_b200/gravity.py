@@ -156,6 +156,18 @@ class GravityTree:
                                                   L.ptr(ninter), L.MEM_HOST))
         return acc, pot, ninter
 
+    def gravity_direct(self, pos, mass, softtype, want_pot: bool = True):
+        """gravity_direct (src/gravity/gravdirect.c:61-257): the given particles on each other by direct
+        summation, what gravity() runs below DIRECT_SUMMATION_THRESHOLD active particles."""
+        pos = np.ascontiguousarray(pos, np.float64)
+        n = len(pos)
+        acc = np.empty((n, 3), np.float64)
+        pot = np.empty(n, np.float64) if want_pot else None
+        self._check(self.lib.gpugrav_gravity_direct(self._ctx, n, L.ptr(pos), L.ptr(np.ascontiguousarray(mass, np.float64)),
+                                                    L.ptr(np.ascontiguousarray(softtype, np.uint8)), L.ptr(acc), L.ptr(pot),
+                                                    L.MEM_HOST))
+        return acc, pot
+
     def compute_grav_accelerations(self, pos, mass, softtype, topnodes=None, pm_acc=None):
         """First-step sequence of compute_grav_accelerations (src/gravity/accel.c:58-80):
         Barnes-Hut pass, OldAcc = |a_tree + a_PM/G| (gravity_force_finalize, accel.c:237-255),

@@ -63,6 +63,9 @@ FLOPS_PER_INTERACTION = 23.0  # convention of the path's roofline
 # particle count (the walk reads the tree and the particles once from DRAM; everything else hits
 # in L2)
 WALK32_DRAM_BYTES_PER_PARTICLE = 362.9e6 / (1 << 21)
+# ErrTolForceAcc of the per-target FP64 walk in the precision ablation: the value at which its RMS
+# error on the zoom box matches the FP32 walk's at 5e-5 (8.1e-4 against 9.3e-4)
+ABLATION_FP64_ALPHA = 2e-5
 
 
 def log(*a):
@@ -681,6 +684,9 @@ def our_arm(args):
     acc_tree = acc_h.numpy()[tg]
 
     def err_stats(acc_dir):
+        return err_stats_of(acc_tree, acc_dir)
+
+    def err_stats_of(acc_tree, acc_dir):
         dn = np.linalg.norm(acc_dir, axis=1)
         err_abs = np.linalg.norm(acc_tree - acc_dir, axis=1)
         rel = err_abs / np.maximum(dn, 1e-300)
@@ -695,6 +701,41 @@ def our_arm(args):
                      reference="FP64 direct sum over pairs closer than Rcut with the exact erfc factor (the range the "
                                "walk evaluates): the tree approximation error",
                      vs_full_short_range=err_stats(acc_full))
+
+    # ---- precision ablation on the same particles and tree code: the FP32 walk's algorithm with FP64
+    # arithmetic, and the per-target FP64 walk (the reference's decisions) at matched accuracy ----
+    ablation = None
+    if prec == L.PREC_FP32 and not args.no_ablation:
+        ablation = {}
+        for name, p_mode, alpha, steps in (("fp64_group_walk", L.PREC_FP64_GROUP, args.err_tol_force_acc, 3),
+                                           ("fp64_per_target_walk", L.PREC_FP64, ABLATION_FP64_ALPHA, 2)):
+            pa = ics.params_for(ic, precision=p_mode, err_tol_theta=0.0, err_tol_force_acc=alpha)
+            tree.set_params(pa)
+            compute(L.ptr(oldacc_d), L.MEM_DEVICE, pos_d, mass_d, st_d, acc_d, pot_d, ni_d)  # warm-up
+            torch.cuda.synchronize()
+            start.record(stream)
+            wl = []
+            for _ in range(steps):
+                compute(L.ptr(oldacc_d), L.MEM_DEVICE, pos_d, mass_d, st_d, acc_d, pot_d, ni_d)
+                wl.append(tree.timings().walk_ms)
+            end.record(stream)
+            torch.cuda.synchronize()
+            ms_a = start.elapsed_time(end) / steps
+            ia_a = tree.timings().interactions
+            acc_a = acc_d.cpu().numpy()[tg]
+            ablation[name] = {"err_tol_force_acc": alpha, "steps": steps, "ms_per_step": ms_a,
+                              "value": n / (ms_a * 1e-3), "walk_ms": float(np.mean(wl)), "interactions_per_particle": ia_a / n,
+                              "accuracy": {k: v for k, v in err_stats_of(acc_a, acc_cut).items() if k in ("rms_rel", "p99_rel")}}
+        v32 = n / (ms * 1e-3)
+        ablation["fp32_over_fp64_group"] = v32 / ablation["fp64_group_walk"]["value"]
+        ablation["fp32_over_fp64_per_target"] = v32 / ablation["fp64_per_target_walk"]["value"]
+        ablation["note"] = ("same particles, device-resident inputs, full step (keys, sort, build, walk); fp64_group_walk: "
+                            "the FP32 walk's groups, opening decisions and interaction lists with FP64 arithmetic, at "
+                            "the same ErrTolForceAcc; fp64_per_target_walk: the per-target FP64 walk (the reference's "
+                            "decisions, bit-exact with it) at the ErrTolForceAcc that brings its RMS error to the FP32 "
+                            "walk's")
+        prm.precision = prec
+        tree.set_params(prm)
 
     # ---- roofline of the walk kernel (device time measured with CUDA events on its stream) ----
     pk = L.C.c_double(0.0)
@@ -729,6 +770,7 @@ def our_arm(args):
         "accuracy": acc_stats,
         "interactions_per_particle": ia / n,
         "pm": pm,
+        "precision_ablation": ablation,
         "tree": {"num_nodes": int(info.num_nodes), "max_depth": int(info.max_depth),
                  "topnodes": int(info.num_topnodes)},
     }
@@ -769,6 +811,7 @@ def main():
     ap.add_argument("--log2-half", type=int, default=23, help="log2 of each species' count (23 -> N=2^24)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-ablation", action="store_true", help="skip the FP64 forms of the walk")
     ap.add_argument("--sharded", action="store_true",
                     help="use the sharded multi-GPU form also with one rank (it is the default for N > 1)")
     ap.add_argument("--serve-requests", type=int, default=160, help="requests in the Poisson serving stream")

@@ -62,8 +62,10 @@ enum
 
 enum
 {
-  GPUGRAV_PREC_FP64 = 0, /* parity walk: reference arithmetic, per-target opening decisions */
-  GPUGRAV_PREC_FP32 = 1  /* fast walk: FP32 arithmetic, FP64 separations, compensated sums */
+  GPUGRAV_PREC_FP64       = 0, /* parity walk: reference arithmetic, per-target opening decisions */
+  GPUGRAV_PREC_FP32       = 1, /* fast walk: FP32 arithmetic, FP64 separations, compensated sums */
+  GPUGRAV_PREC_FP64_GROUP = 2  /* the fast walk's algorithm (groups, interaction lists) in FP64 arithmetic:
+                                  the precision ablation of GPUGRAV_PREC_FP32 (no Ewald-corrected mode) */
 };
 
 /* Run parameters: the All.* fields the path reads. */
@@ -96,8 +98,15 @@ enum
   /* MULTIPLE_NODE_SOFTENING: a node whose largest softening exceeds the target's is used once per
    * softening type with that type's mass (ExtNodes[].mass_per_type) instead of being opened
    * (src/gravity/forcetree_walk.c:296-308, 382-401; src/gravity/forcetree.c:1222-1308) */
-  GPUGRAV_FLAG_MULTIPLE_NODE_SOFTENING = 1
+  GPUGRAV_FLAG_MULTIPLE_NODE_SOFTENING = 1,
+  /* ACTIVATE_MINIMUM_OPENING_ANGLE: the relative criterion's mass test opens a node only if it also
+   * spans more than 0.4 (len > 0.4 r) (src/gravity/forcetree_walk.c:266-271) */
+  GPUGRAV_FLAG_MINIMUM_OPENING_ANGLE = 2,
+  /* ALLOW_DIRECT_SUMMATION: gpugrav_compute of fewer than GPUGRAV_DIRECT_SUMMATION_THRESHOLD particles runs
+   * gpugrav_gravity_direct instead of the tree, as gravity() does (src/gravity/accel.c:103-110) */
+  GPUGRAV_FLAG_ALLOW_DIRECT_SUMMATION = 4
 };
+#define GPUGRAV_DIRECT_SUMMATION_THRESHOLD 3000 /* DIRECT_SUMMATION_THRESHOLD, src/main/allvars.h:245-247 */
 
 /* Domain geometry: the globals set by domain_findExtent (src/domain/domain_box.c:169-196). */
 typedef struct gpugrav_domain
@@ -232,7 +241,9 @@ int32_t gpugrav_set_ewald_table(gpugrav_ctx *ctx, int32_t en, const double *fcor
 int32_t gpugrav_pm_periodic(gpugrav_ctx *ctx, int32_t pmgrid, int64_t n, const double *pos, const double *mass, double *acc,
                             double *pot, int32_t mem);
 
-/* ---- one call: load + build + walk (the drop-in for construct_forcetree + gravity_tree) ---- */
+/* ---- one call: load + build + walk (the drop-in for construct_forcetree + gravity_tree) ----
+ * With GPUGRAV_FLAG_ALLOW_DIRECT_SUMMATION and n < GPUGRAV_DIRECT_SUMMATION_THRESHOLD: gpugrav_gravity_direct
+ * (ninter, if given, is n for every particle); dom, top and oldacc are then unused. */
 int32_t gpugrav_compute(gpugrav_ctx *ctx, int64_t n, const double *pos, const double *mass, const uint8_t *softtype,
                         const float *oldacc, const gpugrav_domain *dom, const gpugrav_topnode *top, int32_t ntop,
                         double *acc, double *pot, int32_t *ninter, int32_t mem);
@@ -264,6 +275,17 @@ enum
   GPUGRAV_DIRECT_CUT  = 1
 };
 int32_t gpugrav_direct(gpugrav_ctx *ctx, int64_t ntargets, const int64_t *targets, int32_t mode, double *acc, double *pot);
+
+/* ---- small-N direct summation (gravity_direct, src/gravity/gravdirect.c:61-257) ----
+ * What gravity() runs instead of the tree when fewer than DIRECT_SUMMATION_THRESHOLD particles are
+ * active (src/gravity/accel.c:103-110): the n given particles (the active ones) attract each other,
+ * every pair with force_evaluate_direct's arithmetic (src/gravity/forcetree_walk.c:557-708: tabulated
+ * short-range factor for TreePM, Ewald correction for a periodic box without PM, spline softening),
+ * summed in the given order -- FP64 results bit-identical to the reference's.  Accelerations without G
+ * and potentials (pot may be NULL) in the given order; one particle gets zero force.  Uses the
+ * context's parameters and replaces its loaded particles (load and build again before a walk). */
+int32_t gpugrav_gravity_direct(gpugrav_ctx *ctx, int64_t n, const double *pos, const double *mass, const uint8_t *softtype,
+                               double *acc, double *pot, int32_t mem);
 
 /* ---- serving loop: many independent isolated systems, continuously batched ----
  * Each submitted request is one isolated N-body system (G = 1 units of the params' softening table)

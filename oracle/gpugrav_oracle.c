@@ -71,7 +71,7 @@ typedef struct
   double erracc;     /* All.ErrTolForceAcc */
   double tnf;        /* All.TopNodeFactor */
   int mdom;          /* All.MultipleDomains */
-  int flags;         /* bit 0: MULTIPLE_NODE_SOFTENING */
+  int flags;         /* bit 0: MULTIPLE_NODE_SOFTENING, bit 1: ACTIVATE_MINIMUM_OPENING_ANGLE */
   double soft[16];   /* All.ForceSoftening[] */
 } or_params;
 
@@ -1107,7 +1107,8 @@ void or_walk(int64_t ntargets, const int64_t *targets, const double *tpos, const
                       no = nextnode[k];
                       continue;
                     }
-                  if(m * len2 > r2 * r2 * aold)
+                  /* ACTIVATE_MINIMUM_OPENING_ANGLE adds a minimum angle to the mass test (forcetree_walk.c:266-271) */
+                  if(m * len2 > r2 * r2 * aold && (!(p->flags & 2) || len2 > r2 * (0.4 * 0.4)))
                     {
                       no = nextnode[k];
                       continue;
@@ -1312,5 +1313,116 @@ void or_direct(int64_t ntargets, const int64_t *targets, int64_t n, const double
       acc_out[3 * q + 2] = az;
       if(pot_out)
         pot_out[q] = pt;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* gravity_direct (src/gravity/gravdirect.c:61-257) with the pair arithmetic */
+/* of force_evaluate_direct (src/gravity/forcetree_walk.c:557-708): the n    */
+/* given (active) particles are both targets and sources, summed in order;  */
+/* tabulated short-range factor (TreePM), Ewald correction (periodic tree),  */
+/* spline softening.  One particle: zero force (gravdirect.c:65-81).         */
+/* ------------------------------------------------------------------------ */
+void or_gravity_direct(int64_t n, const double *pos, const double *mass, const uint8_t *stype, const or_params *p,
+                       double *acc_out, double *pot_out)
+{
+  float tab_f[OR_NTAB + 1], tab_p[OR_NTAB + 1];
+  const int pm    = p->periodic && p->asmth > 0;
+  const int ewald = p->periodic && !pm;
+  if(pm)
+    or_shortrange_table(p->rcut_cells, tab_f, tab_p);
+  const double asmthinv  = pm ? 0.5 / p->asmth : 0.0;
+  const double asmthinv2 = asmthinv * asmthinv;
+  const double asmthfac  = asmthinv * (OR_NTAB / (p->rcut_cells / 2.0));
+  for(int64_t i = 0; i < n; i++)
+    {
+      double acc_x = 0, acc_y = 0, acc_z = 0, pot = 0;
+      if(n > 1)
+        {
+          const double pos_x = pos[3 * i + 0], pos_y = pos[3 * i + 1], pos_z = pos[3 * i + 2];
+          const double h_i   = p->soft[stype[i]];
+          for(int64_t j = 0; j < n; j++)
+            {
+              double h_j  = p->soft[stype[j]];
+              double hmax = (h_j > h_i) ? h_j : h_i;
+              double dx   = nearest(pos[3 * j + 0] - pos_x, p);
+              double dy   = nearest(pos[3 * j + 1] - pos_y, p);
+              double dz   = nearest(pos[3 * j + 2] - pos_z, p);
+              double r2   = dx * dx + dy * dy + dz * dz;
+              double m    = mass[j];
+              double r    = sqrt(r2);
+              double factor_force = 0, factor_pot = 0;
+              if(pm)
+                {
+                  double tabentry = asmthfac * r;
+                  int tabindex    = (int)tabentry;
+                  if(tabindex >= OR_NTAB)
+                    continue;
+                  double tabweight = tabentry - tabindex;
+                  factor_force     = (1.0 - tabweight) * tab_f[tabindex] + tabweight * tab_f[tabindex + 1];
+                  factor_pot       = (1.0 - tabweight) * tab_p[tabindex] + tabweight * tab_p[tabindex + 1];
+                }
+              double fac, wp;
+              if(r >= hmax)
+                {
+                  double rinv  = 1.0 / r;
+                  double rinv3 = rinv * rinv * rinv;
+                  if(pm)
+                    {
+                      fac = rinv3 + rinv * factor_force * asmthinv2;
+                      wp  = rinv * factor_pot;
+                    }
+                  else
+                    {
+                      fac = rinv3;
+                      wp  = -rinv;
+                    }
+                }
+              else
+                {
+                  double h_inv  = 1.0 / hmax;
+                  double h3_inv = h_inv * h_inv * h_inv;
+                  double u      = r * h_inv;
+                  if(u < 0.5)
+                    {
+                      double u2 = u * u;
+                      fac       = h3_inv * (SF1 + u2 * (SF2 * u + SF3));
+                      wp        = h_inv * (SF4 + u2 * (SF5 + u2 * (SF6 * u + SF7)));
+                    }
+                  else
+                    {
+                      double u2 = u * u;
+                      double u3 = u2 * u;
+                      fac       = h3_inv * (SF8 + SF9 * u + SF10 * u2 + SF11 * u3 + SF12 / u3);
+                      wp        = h_inv * (SF13 + SF14 / u + u2 * (SF1 + u * (SF15 + u * (SF16 + SF17 * u))));
+                    }
+                  if(pm && r > 0)
+                    {
+                      double rinv = 1.0 / r;
+                      fac += rinv * factor_force * asmthinv2;
+                      wp += rinv * (factor_pot + 1.0);
+                    }
+                }
+              pot += m * wp;
+              fac *= m;
+              acc_x += dx * fac;
+              acc_y += dy * fac;
+              acc_z += dz * fac;
+              if(ewald)
+                {
+                  double fcorr[3], pcorr;
+                  or_ewald_corr(dx, dy, dz, fcorr, &pcorr);
+                  acc_x += m * fcorr[0];
+                  acc_y += m * fcorr[1];
+                  acc_z += m * fcorr[2];
+                  pot += m * pcorr;
+                }
+            }
+        }
+      acc_out[3 * i + 0] = acc_x;
+      acc_out[3 * i + 1] = acc_y;
+      acc_out[3 * i + 2] = acc_z;
+      if(pot_out)
+        pot_out[i] = pot;
     }
 }

@@ -55,7 +55,7 @@ class OrParams(C.Structure):
         ("erracc", C.c_double),
         ("tnf", C.c_double),
         ("mdom", C.c_int),
-        ("flags", C.c_int),  # bit 0: MULTIPLE_NODE_SOFTENING
+        ("flags", C.c_int),  # bit 0: MULTIPLE_NODE_SOFTENING, bit 1: ACTIVATE_MINIMUM_OPENING_ANGLE
         ("soft", C.c_double * MAX_SOFT),
     ]
 
@@ -86,11 +86,21 @@ def build_ref(ref_root: str = "/root/reference") -> bool:
         subprocess.check_call(
             ["make", "-s", "-j8", "-C", os.path.join(HERE, "ref"), f"REF={ref_root}", f"OUT={REF_DIR}"]
         )
+        # the builds that call the library through its C binding, once the library exists
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "arepo_b200", "libarepo_gpugrav.so")):
+            subprocess.check_call(
+                ["make", "-s", "-j8", "-C", os.path.join(HERE, "ref"), f"REF={ref_root}", f"OUT={REF_DIR}", "gpu"]
+            )
     return ref_available()
 
 
 def ref_available() -> bool:
     return all(os.path.exists(os.path.join(REF_DIR, f"ref_harness_{c}")) for c in ("pm", "iso"))
+
+
+def ref_gpu_available() -> bool:
+    """the harness builds whose gravity step calls the library through its C binding"""
+    return all(os.path.exists(os.path.join(REF_DIR, f"ref_harness_{c}_gpu")) for c in ("pm", "iso"))
 
 
 _lib = None
@@ -115,6 +125,7 @@ def lib():
         _lib.or_mass_per_type.argtypes = [i64, p, i64, p, p, C.c_int, p]
         _lib.or_mass_per_type.restype = C.c_int
         _lib.or_direct.argtypes = [i64, p, i64, p, p, p, p, p, p]
+        _lib.or_gravity_direct.argtypes = [i64, p, p, p, p, p, p]
         _lib.or_ewald_table.argtypes = [p, p, p, p]
         _lib.or_set_ewald_table.argtypes = [C.c_double, p, p, p, p]
     return _lib
@@ -173,6 +184,7 @@ def make_params(
     mdom: int = 8,
     tnf: float = 2.5,
     mns: bool = False,
+    minangle: bool = False,
 ) -> OrParams:
     """softening: Plummer-equivalent epsilon per type; ForceSoftening = 2.8*eps (set_softenings,
     src/gravity/grav_softening.c:92-95) with a trailing zero entry."""
@@ -187,7 +199,7 @@ def make_params(
     p.erracc = erracc
     p.tnf = tnf
     p.mdom = mdom
-    p.flags = 1 if mns else 0
+    p.flags = (1 if mns else 0) | (2 if minangle else 0)
     for i, e in enumerate(softening):
         p.soft[i] = 2.8 * e
     p.soft[len(softening)] = 0.0
@@ -319,6 +331,19 @@ def direct(pos, mass, st, prm, targets):
     return acc, pot
 
 
+def gravity_direct(pos, mass, st, prm):
+    """gravity_direct (gravdirect.c:61-257): the given particles on each other, tabulated short-range
+    factor, in order; what gravity() runs below DIRECT_SUMMATION_THRESHOLD active particles."""
+    use_ewald(prm)
+    pos = np.ascontiguousarray(pos, np.float64)
+    n = len(pos)
+    acc = np.zeros((n, 3))
+    pot = np.zeros(n)
+    lib().or_gravity_direct(n, _ptr(pos), _ptr(np.ascontiguousarray(mass, np.float64)),
+                            _ptr(np.ascontiguousarray(st, np.uint8)), C.byref(prm), _ptr(acc), _ptr(pot))
+    return acc, pot
+
+
 def shortrange_table(rcut_cells: float = 4.5):
     f = np.zeros(NTAB + 1, np.float32)
     p = np.zeros(NTAB + 1, np.float32)
@@ -397,6 +422,8 @@ def read_output(path):
     k = np.frombuffer(out["keys"], np.uint64).reshape(-1, 2)
     r["key_hi"], r["key_lo"] = k[:, 0].copy(), k[:, 1].copy()
     r["top"] = np.frombuffer(out["topnodes"], TOPNODE_DTYPE).copy()
+    if "order_end" in out:
+        r["order_end"] = np.frombuffer(out["order_end"], np.int64)
     if "tree_meta" in out:
         meta = np.frombuffer(out["tree_meta"], np.int64)
         r["tree_meta"] = dict(max_part=int(meta[0]), max_nodes=int(meta[1]), num_nodes=int(meta[2]),
@@ -424,14 +451,24 @@ def read_output(path):
 
 def run_ref(pos, mass, st, periodic, *, box=1.0, asmth=None, rcut=None, theta=0.7, erracc=0.0025,
             softening=(0.01, 0.01), mdom=8, tnf=2.5, passes=2, dump=1, gt=1, first=0, count=None, stride=1,
-            timeout=3600, ewald=False, ewald_table_out=None, mns=False):
+            timeout=3600, ewald=False, ewald_table_out=None, mns=False, gpu=0, active=1, displace=0.0, minangle=False,
+            direct=0):
     """Run the compiled reference harness; returns the parsed dump.  ewald=True: the periodic
     pure-tree build (no PM, Ewald correction); its table file is cached in oracle/_ref/ewald_cache
-    (the reference writes it to the working directory), ewald_table_out dumps the scaled table."""
+    (the reference writes it to the working directory), ewald_table_out dumps the scaled table.
+    gpu=1|2: the harness build whose gravity() step goes through the library's C binding
+    (oracle/ref/gpu_gravity.c) with the FP64 or FP32 walk; active=k: every k-th particle in the active
+    time bin; displace=f: particle 0 moved outside the domain box before the first pass."""
+    if minangle and not (periodic and not ewald and not mns):
+        raise ValueError("the ACTIVATE_MINIMUM_OPENING_ANGLE harness is a periodic TreePM build")
     if mns and not (periodic and not ewald):
         raise ValueError("the MULTIPLE_NODE_SOFTENING harness is a periodic TreePM build")
     exe = os.path.join(REF_DIR, "ref_harness_ewald" if ewald else
-                       ("ref_harness_pm_mns" if mns else ("ref_harness_pm" if periodic else "ref_harness_iso")))
+                       ("ref_harness_pm_mns" if mns else ("ref_harness_pm_mina" if minangle else
+                                                           ("ref_harness_pm" if periodic else "ref_harness_iso"))))
+    if gpu:
+        exe += "_gpu"
+
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
     cwd = None
@@ -444,7 +481,7 @@ def run_ref(pos, mass, st, periodic, *, box=1.0, asmth=None, rcut=None, theta=0.
         eps = list(softening) + [softening[-1]] * (2 - len(softening))
         args = [exe, fin, fout, f"box={box!r}", f"theta={theta!r}", f"erracc={erracc!r}", f"eps0={eps[0]!r}",
                 f"eps1={eps[1]!r}", f"mdom={mdom}", f"tnf={tnf!r}", f"passes={passes}", f"dump={dump}", f"gt={gt}",
-                f"first={first}", f"stride={stride}"]
+                f"first={first}", f"stride={stride}", f"gpu={gpu}", f"active={active}", f"displace={displace!r}", f"direct={direct}"]
         if count is not None:
             args.append(f"count={count}")
         if periodic and not ewald:

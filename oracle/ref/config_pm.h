@@ -5,3 +5,4 @@
 #define EVALPOTENTIAL
 #define DO_NOT_RANDOMIZE_DOMAINCENTER
 #define NSOFTTYPES 2
+#define ALLOW_DIRECT_SUMMATION

@@ -158,10 +158,47 @@ int MPI_Recv(void *b, int n, MPI_Datatype t, int src, int tag, MPI_Comm c, MPI_S
   no_p2p("MPI_Recv");
   return 1;
 }
+/* non-blocking messages to oneself (the only rank): a send is kept until the receive with the same
+ * tag takes it (or the other way round); both are complete once matched */
+#define SELF_MSGS 64
+static struct
+{
+  const void *sbuf;
+  void *rbuf;
+  size_t bytes;
+  int tag, has_send, has_recv;
+} self_msg[SELF_MSGS];
+static void self_match(int k)
+{
+  if(self_msg[k].has_send && self_msg[k].has_recv)
+    {
+      copy_in(self_msg[k].sbuf, self_msg[k].rbuf, self_msg[k].bytes);
+      self_msg[k].has_send = self_msg[k].has_recv = 0;
+    }
+}
+static int self_slot(int tag, int want_send)
+{
+  for(int k = 0; k < SELF_MSGS; k++)
+    if(self_msg[k].tag == tag && (want_send ? (self_msg[k].has_recv && !self_msg[k].has_send)
+                                            : (self_msg[k].has_send && !self_msg[k].has_recv)))
+      return k;
+  for(int k = 0; k < SELF_MSGS; k++)
+    if(!self_msg[k].has_send && !self_msg[k].has_recv)
+      return k;
+  no_p2p("more than 64 pending messages to oneself");
+  return -1;
+}
 int MPI_Isend(const void *b, int n, MPI_Datatype t, int dest, int tag, MPI_Comm c, MPI_Request *rq)
 {
-  no_p2p("MPI_Isend");
-  return 1;
+  if(dest != 0)
+    no_p2p("MPI_Isend to another rank");
+  int k              = self_slot(tag, 1);
+  self_msg[k].sbuf   = b;
+  self_msg[k].tag    = tag;
+  self_msg[k].bytes  = (size_t)n * type_size(t);
+  self_msg[k].has_send = 1;
+  self_match(k);
+  return 0;
 }
 int MPI_Issend(const void *b, int n, MPI_Datatype t, int dest, int tag, MPI_Comm c, MPI_Request *rq)
 {
@@ -170,8 +207,14 @@ int MPI_Issend(const void *b, int n, MPI_Datatype t, int dest, int tag, MPI_Comm
 }
 int MPI_Irecv(void *b, int n, MPI_Datatype t, int src, int tag, MPI_Comm c, MPI_Request *rq)
 {
-  no_p2p("MPI_Irecv");
-  return 1;
+  if(src != 0)
+    no_p2p("MPI_Irecv from another rank");
+  int k              = self_slot(tag, 0);
+  self_msg[k].rbuf   = b;
+  self_msg[k].tag    = tag;
+  self_msg[k].has_recv = 1;
+  self_match(k);
+  return 0;
 }
 int MPI_Wait(MPI_Request *rq, MPI_Status *st) { return 0; }
 int MPI_Waitall(int n, MPI_Request *rq, MPI_Status *st) { return 0; }

@@ -29,7 +29,15 @@
  *             the particles and the tree copy-on-write; targets dealt round-robin),
  *             reps (after the last pass, walk the selected targets that many more times and
  *             print each walk's wall time: the CPU timing of a bounded sample),
- *             lite (1 = write only the timing sections, not the per-particle arrays)
+ *             lite (1 = write only the timing sections, not the per-particle arrays),
+ *             active (k > 1: only every k-th particle, in P[] order, is in the active gravity time
+ *             bin, so gravity_tree walks that TargetList), displace (f != 0: before the first
+ *             pass, particle 0 is moved to DomainCorner + (1 + f) DomainLen in x, outside the domain
+ *             box: the tree build's -3 recovery), gpu (harness builds with GPU_GRAVITY only: 1 or 2
+ *             replaces construct_forcetree + gravity_tree by the library's FP64 or FP32 walk through
+ *             gpu_gravity.c, the binding AREPO would use), direct (1 = gravity_direct, the
+ *             direct summation gravity() runs below DIRECT_SUMMATION_THRESHOLD active particles,
+ *             instead of the tree; builds with ALLOW_DIRECT_SUMMATION)
  */
 #include <math.h>
 #include <stdint.h>
@@ -44,6 +52,23 @@
 #include "allvars.h"
 #include "proto.h"
 #include "../domain/domain.h"
+
+#ifdef GPU_GRAVITY
+#include "gpugrav.h"
+int gpu_gravity_tree(int timebin, int precision);
+void gpu_gravity_free(void);
+#endif
+
+/* only every k-th particle active in the gravity time bin: gravity_tree's TargetList
+ * (gravity/gravtree.c:494-520) is built from this list */
+static void set_active_every(int k)
+{
+  int m = 0;
+  for(int i = 0; i < NumPart; i += k)
+    TimeBinsGravity.ActiveParticleList[m++] = i;
+  TimeBinsGravity.NActiveParticles       = m;
+  TimeBinsGravity.GlobalNActiveParticles = m;
+}
 
 static double wall(void)
 {
@@ -261,6 +286,24 @@ int main(int argc, char **argv)
   int lite   = (int)arg_d(argc, argv, "lite", 0);
   if(procs < 1)
     procs = 1;
+  int active      = (int)arg_d(argc, argv, "active", 1);
+  double displace = arg_d(argc, argv, "displace", 0.0);
+  int use_gpu     = (int)arg_d(argc, argv, "gpu", 0);
+  int use_direct  = (int)arg_d(argc, argv, "direct", 0);
+#ifndef ALLOW_DIRECT_SUMMATION
+  if(use_direct)
+    {
+      fprintf(stderr, "ref_harness: direct=1 needs a build with ALLOW_DIRECT_SUMMATION\n");
+      return 1;
+    }
+#endif
+#ifndef GPU_GRAVITY
+  if(use_gpu)
+    {
+      fprintf(stderr, "ref_harness: gpu=%d needs a GPU_GRAVITY build (ref_harness_*_gpu)\n", use_gpu);
+      return 1;
+    }
+#endif
   if(first < 0 || first > n)
     first = 0;
   if(count < 0 || first + count > n)
@@ -410,19 +453,63 @@ int main(int argc, char **argv)
 
   for(int pass = 0; pass < passes; pass++)
     {
+      if(pass == 0 && displace != 0)
+        P[0].Pos[0] = DomainCorner[0] + DomainLen * (1.0 + displace);
+      if(active > 1)
+        set_active_every(active);
+      memset(acc, 0, sizeof(double) * 3 * n);
+      memset(pot, 0, sizeof(double) * n);
+      memset(ninter, 0, sizeof(int) * n);
+      double t_build = 0, t_walk = 0, t_gt = 0;
+#ifdef GPU_GRAVITY
+      if(use_gpu)
+        {
+          for(int i = 0; i < n; i++)
+            for(int k = 0; k < 3; k++)
+              P[i].GravAccel[k] = 0;
+          double tg0     = wall();
+          int recoveries = gpu_gravity_tree(bin, use_gpu == 2 ? GPUGRAV_PREC_FP32 : GPUGRAV_PREC_FP64);
+          t_gt           = wall() - tg0;
+          for(int i = 0; i < n; i++)
+            {
+              for(int k = 0; k < 3; k++)
+                gacc[3 * i + k] = acc[3 * i + k] = P[i].GravAccel[k];
+#ifdef EVALPOTENTIAL
+              pot[i] = P[i].Potential;
+#endif
+            }
+          printf("gpu pass=%d recoveries=%d time=%.6f\n", pass, recoveries, t_gt);
+        }
+      else
+#endif
+#ifdef ALLOW_DIRECT_SUMMATION
+          if(use_direct)
+        {
+          double td0 = wall();
+          gravity_direct(bin);
+          t_gt = wall() - td0;
+          for(int i = 0; i < n; i++)
+            {
+              for(int k = 0; k < 3; k++)
+                gacc[3 * i + k] = acc[3 * i + k] = P[i].GravAccel[k];
+#ifdef EVALPOTENTIAL
+              pot[i] = P[i].Potential;
+#endif
+            }
+        }
+      else
+#endif
+        {
       double tb0 = wall();
       construct_forcetree(0, 1, 0, bin);
-      double t_build = wall() - tb0;
+      t_build = wall() - tb0;
 
       if(dump && pass == 0)
         dump_tree(fo);
 
-      memset(acc, 0, sizeof(double) * 3 * n);
-      memset(pot, 0, sizeof(double) * n);
-      memset(ninter, 0, sizeof(int) * n);
-      double t_walk = walk_targets(first, count, stride, procs, acc, pot, ninter);
+      if(active <= 1)
+        t_walk = walk_targets(first, count, stride, procs, acc, pot, ninter);
 
-      double t_gt = 0;
       if(run_gt)
         {
           double tg0 = wall();
@@ -434,9 +521,10 @@ int main(int argc, char **argv)
         }
       else if(All.TypeOfOpeningCriterion == 1)
         All.ErrTolTheta = 0; /* what gravity_tree() does at its end (gravity/gravtree.c:654-655) */
+        }
 
       /* the bounded CPU timing: the same walk again, reps times, after the last pass's */
-      for(int r = 0; pass == passes - 1 && r < reps; r++)
+      for(int r = 0; !use_gpu && !use_direct && pass == passes - 1 && r < reps; r++)
         {
           double tr     = walk_targets(first, count, stride, procs, acc, pot, ninter);
           long long nir = 0;
@@ -458,14 +546,14 @@ int main(int argc, char **argv)
       snprintf(nm, sizeof(nm), "ninter%d", pass);
       wsec(fo, nm, (int64_t)na * 4);
       wr(fo, ninter, 4, na);
-      if(run_gt)
+      if(run_gt || use_gpu || use_direct)
         {
           snprintf(nm, sizeof(nm), "gacc%d", pass);
           wsec(fo, nm, (int64_t)n * 24);
           wr(fo, gacc, 8, 3 * (size_t)n);
         }
 
-      if(!run_gt)
+      if(!run_gt && !use_gpu && !use_direct)
         {
           /* store the walk results where gravity_tree() would have put them */
           for(int i = 0; i < n; i++)
@@ -473,7 +561,8 @@ int main(int argc, char **argv)
               P[i].GravAccel[k] = acc[3 * i + k];
         }
       gravity_force_finalize(bin);
-      free_tree();
+      if(!use_gpu && !use_direct)
+        free_tree();
 
       snprintf(nm, sizeof(nm), "oldacc%d", pass);
       wsec(fo, nm, (int64_t)na * 4);
@@ -495,6 +584,16 @@ int main(int argc, char **argv)
              t_domain, t_build, t_walk, nt, nint, t_gt);
     }
 
+  /* particle order after the passes (a -3 recovery redoes the domain decomposition) */
+  wsec(fo, "order_end", (int64_t)n * 8);
+  for(int i = 0; i < n; i++)
+    {
+      int64_t o = (int64_t)P[i].ID - 1;
+      wr(fo, &o, 8, 1);
+    }
+#ifdef GPU_GRAVITY
+  gpu_gravity_free();
+#endif
   wsec(fo, "end", 0);
   fclose(fo);
   return 0;

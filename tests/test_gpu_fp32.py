@@ -141,3 +141,22 @@ def test_fp32_walk_multiple_node_softening(cuda_lib):
     rel32, glob32 = _err(out[L.PREC_FP32][0][tg], d)
     assert glob32 <= glob64 * 1.02 + 2e-5, (glob32, glob64)
     assert rel32 <= rel64 * 1.02 + 2e-5, (rel32, rel64)
+
+
+@pytest.mark.parametrize("name", ["zoom", "hernquist"])
+def test_fp64_group_walk_is_the_fp32_walk_in_double(name, cuda_lib):
+    """GPUGRAV_PREC_FP64_GROUP runs the FP32 walk's algorithm (same groups, same opening decisions, same
+    interaction lists) with FP64 arithmetic: it differs from the FP32 walk by FP32 rounding only, and
+    is no less accurate than the FP64 parity walk against the direct sum."""
+    ic = CASES[name]()
+    n = len(ic["mass"])
+    tg = np.sort(np.random.default_rng(6).choice(n, 2048, replace=False))
+    a32, _, n32, d = _run(ic, L.PREC_FP32, tg)
+    ag, _, ng, _ = _run(ic, L.PREC_FP64_GROUP, tg)
+    a64, _, _, _ = _run(ic, L.PREC_FP64, tg)
+    scale = np.sqrt(np.mean(np.sum(ag * ag, axis=1)))
+    assert np.sqrt(np.mean(np.sum((a32 - ag) ** 2, axis=1))) / scale < 1e-5
+    assert abs(int(ng.sum()) - int(n32.sum())) <= 1e-5 * int(n32.sum())  # pairs at Rcut may round either way
+    _, glob64 = _err(a64[tg], d)
+    _, globg = _err(ag[tg], d)
+    assert globg <= glob64 * 1.02 + 2e-5, (globg, glob64)

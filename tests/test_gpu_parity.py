@@ -5,6 +5,8 @@ checks compare with the C oracle, which the CPU tests pin bit-for-bit to the
 same fixtures.  The FP64 path must reproduce keys, order, top tree, tree
 (reference node numbering) and per-particle accelerations, potentials and
 interaction counts bit for bit."""
+import os
+
 import numpy as np
 import pytest
 
@@ -220,3 +222,29 @@ def test_error_codes(cuda_lib):
         t.construct_forcetree(topnodes=g["top"])
         acc, _, _ = t.gravity_tree()
         assert np.array_equal(acc[g["order"]], g["acc0"])
+
+
+def test_minimum_opening_angle_bitexact(cuda_lib):
+    """ACTIVATE_MINIMUM_OPENING_ANGLE (GPUGRAV_FLAG_MINIMUM_OPENING_ANGLE): both passes bit-exact with
+    the C oracle, which is pinned to a harness build of the reference with that option where it is built;
+    the FP32 walk with the flag stays no less accurate than the FP64 walk."""
+    ic = _live_case("zoom", 32768, 51)
+    soft = tuple(ic["softening"])
+    p = dict(periodic=True, box=1.0, asmth=ic["asmth"], rcut=ic["rcut"], rcut_cells=4.5, softening=soft, theta=0.7,
+             erracc=0.0025, mdom=8, tnf=2.5)
+    op = oracle_params(p)
+    op.flags |= 2
+    ref = O.pipeline(ic["pos"], ic["mass"], ic["softtype"], op)
+    order = ref["perm"]
+    prm = gpu_params(p)
+    prm.flags |= L.FLAG_MINIMUM_OPENING_ANGLE
+    with GravityTree(prm) as t:
+        acc, pot, ni, oldacc = t.compute_grav_accelerations(ic["pos"], ic["mass"], ic["softtype"])
+    assert np.array_equal(oldacc[order], ref["oldacc0"])
+    assert np.array_equal(acc[order], ref["acc1"]) and np.array_equal(ni[order], ref["ninter1"])
+    plain = O.pipeline(ic["pos"], ic["mass"], ic["softtype"], oracle_params(p))
+    assert ref["ninter1"].sum() < plain["ninter1"].sum()  # the option opens fewer nodes
+    if O.ref_available() and os.path.exists(os.path.join(O.REF_DIR, "ref_harness_pm_mina")):
+        r = O.run_ref(ic["pos"], ic["mass"], ic["softtype"], True, asmth=ic["asmth"], rcut=ic["rcut"], softening=soft,
+                      dump=0, gt=0, minangle=True)
+        assert np.array_equal(r["acc1"], ref["acc1"]) and np.array_equal(r["ninter1"], ref["ninter1"])

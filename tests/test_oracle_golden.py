@@ -104,3 +104,23 @@ def test_oracle_walk_close_to_direct_sum(name):
     scale = np.sqrt(np.mean(np.sum(acc_d * acc_d, axis=1)))
     err = np.linalg.norm(acc_t - acc_d, axis=1) / scale
     assert np.sqrt(np.mean(err ** 2)) < 2e-2
+
+
+def test_oracle_minimum_opening_angle_matches_reference_build():
+    """The oracle's ACTIVATE_MINIMUM_OPENING_ANGLE flag against a harness build of the reference with that
+    option (oracle/ref/config_pm_mina.h), both passes bit for bit; skipped where the harness is not built."""
+    import os
+
+    if not os.path.exists(os.path.join(O.REF_DIR, "ref_harness_pm_mina")):
+        pytest.skip("reference harness with ACTIVATE_MINIMUM_OPENING_ANGLE not built")
+    from arepo_b200 import ics
+
+    ic = ics.zoom_box(log2_half=12, seed=52, pmgrid=64)
+    soft = tuple(ic["softening"])
+    prm = O.make_params(True, asmth=ic["asmth"], rcut=ic["rcut"], softening=soft, minangle=True)
+    out = O.pipeline(ic["pos"], ic["mass"], ic["softtype"], prm)
+    r = O.run_ref(ic["pos"], ic["mass"], ic["softtype"], True, asmth=ic["asmth"], rcut=ic["rcut"], softening=soft, dump=0,
+                  gt=0, minangle=True)
+    assert np.array_equal(out["perm"], r["order"])
+    for ps in (0, 1):
+        assert np.array_equal(out[f"acc{ps}"], r[f"acc{ps}"]) and np.array_equal(out[f"ninter{ps}"], r[f"ninter{ps}"])
