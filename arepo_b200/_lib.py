@@ -67,6 +67,25 @@ class Params(C.Structure):
     ]
 
 
+class TimestepParams(C.Structure):
+    """gpugrav_timestep_params: the All.* fields of get_timestep_gravity (timestep.c:284-353)."""
+    _fields_ = [
+        ("err_tol_int_accuracy", C.c_double),
+        ("cf_atime", C.c_double),
+        ("cf_a2inv", C.c_double),
+        ("cf_hubble_a", C.c_double),
+        ("max_size_timestep", C.c_double),
+        ("min_size_timestep", C.c_double),
+        ("dt_displacement", C.c_double),
+        ("timebase_interval", C.c_double),
+        ("timebase", C.c_int64),
+        ("ti_current", C.c_int64),
+        ("nostop_below_min", C.c_int32),
+        ("pad", C.c_int32),
+        ("synchronized", C.c_uint8 * 64),
+    ]
+
+
 class Domain(C.Structure):
     _fields_ = [
         ("corner", C.c_double * 3),
@@ -171,6 +190,8 @@ _SIGS = {
     "gpugrav_walk": (C.c_int32, [_P, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_walk_targets": (C.c_int32, [_P, C.c_int64, _P, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_gravity_direct": (C.c_int32, [_P, C.c_int64, _P, _P, _P, _P, _P, C.c_int32]),
+    "gpugrav_timestep_gravity": (C.c_int32, [_P, _P, C.c_int64, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_int32]),
+    "gpugrav_active_particles": (C.c_int32, [_P, C.c_int64, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_set_target_slice": (C.c_int32, [_P, C.c_int32, C.c_int32]),
     "gpugrav_pm_periodic": (C.c_int32, [_P, C.c_int32, C.c_int64, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_set_ewald_table": (C.c_int32, [_P, C.c_int32, _P, _P, _P, _P]),

@@ -30,6 +30,7 @@ SOURCES = [
     ("direct_noalloc.cu", True),
     ("walk32.cu", False),
     ("targets.cu", False),
+    ("timestep.cu", True),
     ("peak.cu", False),
     ("serve.cu", False),
     ("pm.cu", False),

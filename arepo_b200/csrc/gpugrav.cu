@@ -865,6 +865,107 @@ int32_t gpugrav_walk_targets(gpugrav_ctx *c, int64_t ntargets, const int32_t *ta
   return walk_impl(c, ntargets, targets ? targets : &none, oldacc, acc, pot, ninter, mem);
 }
 
+int32_t gpugrav_timestep_gravity(gpugrav_ctx *c, const gpugrav_timestep_params *tp, int64_t n, const double *grav_accel,
+                                 const double *grav_pm, const double *mass, const uint64_t *ids, const uint8_t *softtype,
+                                 const int8_t *bin_old, int64_t *ti_step, int8_t *bin, int64_t *failed, int32_t mem)
+{
+  if(!c)
+    return GPUGRAV_ERR_INVALID;
+  if(!tp || n < 1 || !grav_accel || !mass || !softtype || !bin_old || !ti_step || !bin || !(tp->timebase_interval > 0) ||
+     tp->timebase < 2 || (mem != GPUGRAV_MEM_HOST && mem != GPUGRAV_MEM_DEVICE))
+    return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_timestep_gravity: invalid arguments");
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->stream;
+  const double *d_acc = grav_accel, *d_pm = grav_pm, *d_mass = mass;
+  const uint64_t *d_ids = ids;
+  const uint8_t *d_st = softtype;
+  const int8_t *d_bo  = bin_old;
+  int64_t *d_ti       = ti_step;
+  int8_t *d_bin       = bin;
+  gg::DevBuf tmp;
+  if(mem == GPUGRAV_MEM_HOST)
+    {
+      // one staging block: acc | pm | mass | ids | ti | softtype | bin_old | bin
+      const size_t need = n * (24 + (grav_pm ? 24 : 0) + 8 + (ids ? 8 : 0) + 8 + 3) + 256;
+      if(tmp.ensure(need) != cudaSuccess)
+        return fail(c, GPUGRAV_ERR_OOM, "gpugrav_timestep_gravity: device allocation");
+      char *q = tmp.as<char>();
+      auto take = [&](size_t b) { char *r = q; q += (b + 15) & ~(size_t)15; return r; };
+      double *a = (double *)take(n * 24), *pm = grav_pm ? (double *)take(n * 24) : nullptr, *m = (double *)take(n * 8);
+      uint64_t *id = ids ? (uint64_t *)take(n * 8) : nullptr;
+      d_ti         = (int64_t *)take(n * 8);
+      uint8_t *s   = (uint8_t *)take(n);
+      int8_t *bo = (int8_t *)take(n), *bn = (int8_t *)take(n);
+      CK(cudaMemcpyAsync(a, grav_accel, n * 24, cudaMemcpyHostToDevice, st), "upload");
+      if(pm)
+        CK(cudaMemcpyAsync(pm, grav_pm, n * 24, cudaMemcpyHostToDevice, st), "upload");
+      CK(cudaMemcpyAsync(m, mass, n * 8, cudaMemcpyHostToDevice, st), "upload");
+      if(id)
+        CK(cudaMemcpyAsync(id, ids, n * 8, cudaMemcpyHostToDevice, st), "upload");
+      CK(cudaMemcpyAsync(s, softtype, n, cudaMemcpyHostToDevice, st), "upload");
+      CK(cudaMemcpyAsync(bo, bin_old, n, cudaMemcpyHostToDevice, st), "upload");
+      d_acc = a, d_pm = pm, d_mass = m, d_ids = id, d_st = s, d_bo = bo, d_bin = bn;
+    }
+  int code = 0;
+  int64_t first = -1;
+  CK(gg::timestep_stage(c, tp, n, d_acc, d_pm, d_mass, d_ids, d_st, d_bo, d_ti, d_bin, &code, &first), "time steps");
+  if(mem == GPUGRAV_MEM_HOST)
+    {
+      CK(cudaMemcpyAsync(ti_step, d_ti, n * 8, cudaMemcpyDeviceToHost, st), "download");
+      CK(cudaMemcpyAsync(bin, d_bin, n, cudaMemcpyDeviceToHost, st), "download");
+      CK(cudaStreamSynchronize(st), "time steps");
+    }
+  tmp.release();
+  if(failed)
+    *failed = code ? first : -1;
+  static const char *what[] = {"", "time step below MinSizeTimestep", "integer time step outside (0, TIMEBASE)",
+                               "time step of integer size 1", "time step beyond the end of the timeline",
+                               "softening type >= nsofttypes"};
+  if(code)
+    return fail(c, GPUGRAV_ERR_INVALID, what[code < 6 ? code : 0]);
+  return GPUGRAV_OK;
+}
+
+int32_t gpugrav_active_particles(gpugrav_ctx *c, int64_t n, const int8_t *bin, const uint8_t *synchronized, int32_t *list,
+                                 int64_t *count, int32_t mem)
+{
+  if(!c)
+    return GPUGRAV_ERR_INVALID;
+  if(n < 1 || n >= (int64_t)1 << 31 || !bin || !synchronized || !list || !count || (mem != GPUGRAV_MEM_HOST && mem != GPUGRAV_MEM_DEVICE))
+    return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_active_particles: invalid arguments");
+  DeviceGuard g(c->device);
+  cudaStream_t st = c->stream;
+  gg::DevBuf tmp;
+  const size_t need = n * 5 + 256;
+  if(tmp.ensure(need) != cudaSuccess)
+    return fail(c, GPUGRAV_ERR_OOM, "gpugrav_active_particles: device allocation");
+  uint8_t *d_sync  = tmp.as<uint8_t>();
+  int64_t *d_count = (int64_t *)(tmp.as<char>() + 64);
+  const int8_t *d_bin = bin;
+  int32_t *d_list     = list;
+  if(mem == GPUGRAV_MEM_HOST)
+    {
+      int8_t *b = (int8_t *)(tmp.as<char>() + 128);
+      d_list    = (int32_t *)(tmp.as<char>() + 128 + ((n + 15) & ~(int64_t)15));
+      CK(cudaMemcpyAsync(b, bin, n, cudaMemcpyHostToDevice, st), "upload bins");
+      d_bin = b;
+    }
+  CK(cudaMemcpyAsync(d_sync, synchronized, 64, cudaMemcpyHostToDevice, st), "upload synchronized bins");
+  CK(cudaMemsetAsync(d_count, 0, 8, st), "reset count");
+  CK(gg::active_stage(c, n, d_bin, d_sync, d_list, d_count), "active particles");
+  int64_t cnt = 0;
+  CK(cudaMemcpyAsync(&cnt, d_count, 8, cudaMemcpyDeviceToHost, st), "download count");
+  CK(cudaStreamSynchronize(st), "active particles");
+  if(mem == GPUGRAV_MEM_HOST && cnt > 0)
+    {
+      CK(cudaMemcpyAsync(list, d_list, cnt * 4, cudaMemcpyDeviceToHost, st), "download list");
+      CK(cudaStreamSynchronize(st), "active particles");
+    }
+  tmp.release();
+  *count = cnt;
+  return GPUGRAV_OK;
+}
+
 int32_t gpugrav_gravity_direct(gpugrav_ctx *c, int64_t n, const double *pos, const double *mass, const uint8_t *softtype,
                                double *acc, double *pot, int32_t mem)
 {

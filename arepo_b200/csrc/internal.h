@@ -260,6 +260,10 @@ cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc);
 cudaError_t walk32_prepare(gpugrav_ctx *c, const WalkConst &wc);
 cudaError_t walk32_launch(gpugrav_ctx *c);
 cudaError_t groups_stage(gpugrav_ctx *c);
+cudaError_t timestep_stage(gpugrav_ctx *c, const gpugrav_timestep_params *tp, int64_t n, const double *acc, const double *pm,
+                           const double *mass, const uint64_t *ids, const uint8_t *st, const int8_t *bin_old, int64_t *ti,
+                           int8_t *bin, int *fail_code, int64_t *first);
+cudaError_t active_stage(gpugrav_ctx *c, int64_t n, const int8_t *bin, const uint8_t *d_sync, int32_t *list, int64_t *d_count);
 cudaError_t targets_stage(gpugrav_ctx *c, int64_t nt, const int32_t *d_targets, int *flags);
 cudaError_t groups_active_stage(gpugrav_ctx *c, int64_t nt, int cap);
 cudaError_t targets_scatter(gpugrav_ctx *c, int64_t nt, int64_t a, int64_t b, double *acc, double *pot, int32_t *nint);

@@ -168,6 +168,32 @@ class GravityTree:
                                                     L.MEM_HOST))
         return acc, pot
 
+    def timestep_gravity(self, tp: L.TimestepParams, grav_accel, mass, softtype, bin_old, grav_pm=None, ids=None):
+        """get_timestep_gravity + the new TimeBinGrav (timestep.c:284-353, 725-770) per particle:
+        returns (ti_step int64, bin int8)."""
+        a = np.ascontiguousarray(grav_accel, np.float64)
+        n = len(a)
+        ti = np.empty(n, np.int64)
+        b = np.empty(n, np.int8)
+        failed = C.c_int64(-1)
+        pm = None if grav_pm is None else np.ascontiguousarray(grav_pm, np.float64)
+        idv = None if ids is None else np.ascontiguousarray(ids, np.uint64)
+        self._check(self.lib.gpugrav_timestep_gravity(self._ctx, C.byref(tp), n, L.ptr(a), L.ptr(pm),
+                                                      L.ptr(np.ascontiguousarray(mass, np.float64)), L.ptr(idv),
+                                                      L.ptr(np.ascontiguousarray(softtype, np.uint8)),
+                                                      L.ptr(np.ascontiguousarray(bin_old, np.int8)), L.ptr(ti), L.ptr(b),
+                                                      C.byref(failed), L.MEM_HOST))
+        return ti, b
+
+    def active_particles(self, bins, synchronized):
+        """indices of the particles whose time bin is synchronized (TimeBinsGravity.ActiveParticleList)"""
+        b = np.ascontiguousarray(bins, np.int8)
+        sync = (C.c_uint8 * 64)(*[1 if s else 0 for s in synchronized])
+        out = np.empty(len(b), np.int32)
+        cnt = C.c_int64(0)
+        self._check(self.lib.gpugrav_active_particles(self._ctx, len(b), L.ptr(b), sync, L.ptr(out), C.byref(cnt), L.MEM_HOST))
+        return out[: cnt.value].copy()
+
     def compute_grav_accelerations(self, pos, mass, softtype, topnodes=None, pm_acc=None):
         """First-step sequence of compute_grav_accelerations (src/gravity/accel.c:58-80):
         Barnes-Hut pass, OldAcc = |a_tree + a_PM/G| (gravity_force_finalize, accel.c:237-255),

@@ -287,6 +287,43 @@ int32_t gpugrav_direct(gpugrav_ctx *ctx, int64_t ntargets, const int64_t *target
 int32_t gpugrav_gravity_direct(gpugrav_ctx *ctx, int64_t n, const double *pos, const double *mass, const uint8_t *softtype,
                                double *acc, double *pot, int32_t mem);
 
+/* ---- gravity time steps and time bins (src/time_integration/timestep.c) ----
+ * get_timestep_gravity (timestep.c:284-353) for every particle, then the bin of
+ * timebins_get_bin_and_do_validity_checks (timestep.c:725-770): the step rounded down to a power of two
+ * of the integer timeline, raised only into synchronized bins, 0 at the end of the timeline.  Then the
+ * list of active particles of a time bin (TimeBinsGravity.ActiveParticleList for the bins that are
+ * synchronized now), ready for gpugrav_walk_targets.  Parameters are AREPO's All.* fields; the
+ * softening lengths come from the context (ForceSoftening). */
+typedef struct gpugrav_timestep_params
+{
+  double err_tol_int_accuracy;       /* All.ErrTolIntAccuracy */
+  double cf_atime, cf_a2inv, cf_hubble_a; /* All.cf_* (1 without comoving integration) */
+  double max_size_timestep;          /* All.MaxSizeTimestep */
+  double min_size_timestep;          /* All.MinSizeTimestep */
+  double dt_displacement;            /* All.DtDisplacement (PMGRID builds); 0: no such limit */
+  double timebase_interval;          /* All.Timebase_interval */
+  int64_t timebase;                  /* TIMEBASE of the build (1 << TIMEBINS) */
+  int64_t ti_current;                /* All.Ti_Current */
+  int32_t nostop_below_min;          /* NOSTOP_WHEN_BELOW_MINTIMESTEP: clamp instead of failing */
+  int32_t pad;
+  uint8_t synchronized[64];          /* TimeBinSynchronized[bin] */
+} gpugrav_timestep_params;
+
+/* grav_accel: n*3 accelerations as gravity_force_finalize leaves them (with G); grav_pm: n*3 (PMGRID) or
+ * NULL; ids: P[].ID or NULL (a particle with mass 0 and ID 0 takes the maximum step); bin_old: the
+ * current TimeBinGrav of each particle.  Outputs ti_step (integer steps before the power-of-two
+ * rounding, as get_timestep_gravity returns them) and bin (the new TimeBinGrav).  Errors the reference
+ * stops on: GPUGRAV_ERR_INVALID (a step below MinSizeTimestep without nostop_below_min, an integer step
+ * outside (0, TIMEBASE), a step of integer size 1, a step beyond the end of the timeline); `failed`
+ * (may be NULL) receives the first failing particle. */
+int32_t gpugrav_timestep_gravity(gpugrav_ctx *ctx, const gpugrav_timestep_params *tp, int64_t n, const double *grav_accel,
+                                 const double *grav_pm, const double *mass, const uint64_t *ids, const uint8_t *softtype,
+                                 const int8_t *bin_old, int64_t *ti_step, int8_t *bin, int64_t *failed, int32_t mem);
+/* Particles whose bin is synchronized (synchronized[bin] != 0), in index order: list (capacity n) and
+ * their count. */
+int32_t gpugrav_active_particles(gpugrav_ctx *ctx, int64_t n, const int8_t *bin, const uint8_t *synchronized, int32_t *list,
+                                 int64_t *count, int32_t mem);
+
 /* ---- serving loop: many independent isolated systems, continuously batched ----
  * Each submitted request is one isolated N-body system (G = 1 units of the params' softening table)
  * that runs what the reference runs on its first step and afterwards: a Barnes-Hut force pass

@@ -1426,3 +1426,87 @@ void or_gravity_direct(int64_t n, const double *pos, const double *mass, const u
         pot_out[i] = pot;
     }
 }
+
+/* ------------------------------------------------------------------------ */
+/* get_timestep_gravity (src/time_integration/timestep.c:284-353) and the    */
+/* bin of timebins_get_bin_and_do_validity_checks (timestep.c:725-770).      */
+/* Returns 0, or the reference's stop: 1 below MinSizeTimestep, 2 integer    */
+/* step outside (0, TIMEBASE), 3 integer step 1, 4 beyond the end of the     */
+/* timeline.                                                                 */
+/* ------------------------------------------------------------------------ */
+typedef struct
+{
+  double eta, cf_atime, cf_a2inv, cf_hubble_a, dtmax, dtmin, dtdisp, timebase_interval;
+  int64_t timebase, ti_current;
+  int nostop;
+  int pad;
+  unsigned char sync[64];
+} or_tsparams;
+
+int or_timestep_gravity(int64_t n, const double *acc, const double *pm, const double *mass, const uint64_t *ids,
+                        const uint8_t *stype, const or_params *p, const or_tsparams *t, const int8_t *bin_old, int64_t *ti_out,
+                        int8_t *bin_out)
+{
+  int err = 0;
+  for(int64_t i = 0; i < n; i++)
+    {
+      double ax = t->cf_a2inv * acc[3 * i + 0], ay = t->cf_a2inv * acc[3 * i + 1], az = t->cf_a2inv * acc[3 * i + 2];
+      if(pm)
+        {
+          ax += t->cf_a2inv * pm[3 * i + 0];
+          ay += t->cf_a2inv * pm[3 * i + 1];
+          az += t->cf_a2inv * pm[3 * i + 2];
+        }
+      double ac = sqrt(ax * ax + ay * ay + az * az);
+      if(ac == 0)
+        ac = 1.0e-30;
+      double dt = sqrt(2 * t->eta * t->cf_atime * p->soft[stype[i]] / 2.8 / ac);
+      dt *= t->cf_hubble_a;
+      if(mass[i] == 0 && ids && ids[i] == 0)
+        dt = t->dtmax;
+      if(dt >= t->dtmax)
+        dt = t->dtmax;
+      if(dt < t->dtmin)
+        {
+          if(t->nostop)
+            dt = t->dtmin;
+          else if(!err)
+            err = 1;
+        }
+      if(t->dtdisp > 0 && dt >= t->dtdisp)
+        dt = t->dtdisp;
+      int64_t ti = t->timebase <= ((int64_t)1 << 30) ? (int64_t)(int)(dt / t->timebase_interval) : (int64_t)(dt / t->timebase_interval);
+      if(!(ti > 0 && ti < t->timebase) && !err)
+        err = 2;
+      ti_out[i]      = ti;
+      int64_t ti_min = t->timebase;
+      while(ti_min > ti)
+        ti_min >>= 1;
+      int64_t ts = ti_min;
+      int bin    = -1;
+      if(ts == 0)
+        bin = 0;
+      if(ts == 1 && !err)
+        err = 3;
+      while(ts)
+        {
+          bin++;
+          ts >>= 1;
+        }
+      if(bin > bin_old[i])
+        {
+          while(bin > bin_old[i] && !t->sync[bin])
+            bin--;
+          ts = bin ? ((int64_t)1 << bin) : 0;
+        }
+      if(t->ti_current >= t->timebase)
+        {
+          ts  = 0;
+          bin = 0;
+        }
+      if(t->timebase - t->ti_current < ts && !err)
+        err = 4;
+      bin_out[i] = (int8_t)bin;
+    }
+  return err;
+}

@@ -126,6 +126,8 @@ def lib():
         _lib.or_mass_per_type.restype = C.c_int
         _lib.or_direct.argtypes = [i64, p, i64, p, p, p, p, p, p]
         _lib.or_gravity_direct.argtypes = [i64, p, p, p, p, p, p]
+        _lib.or_timestep_gravity.argtypes = [i64, p, p, p, p, p, p, p, p, p, p]
+        _lib.or_timestep_gravity.restype = C.c_int
         _lib.or_ewald_table.argtypes = [p, p, p, p]
         _lib.or_set_ewald_table.argtypes = [C.c_double, p, p, p, p]
     return _lib
@@ -344,6 +346,34 @@ def gravity_direct(pos, mass, st, prm):
     return acc, pot
 
 
+class OrTsParams(C.Structure):
+    _fields_ = [("eta", C.c_double), ("cf_atime", C.c_double), ("cf_a2inv", C.c_double), ("cf_hubble_a", C.c_double),
+                ("dtmax", C.c_double), ("dtmin", C.c_double), ("dtdisp", C.c_double), ("timebase_interval", C.c_double),
+                ("timebase", C.c_int64), ("ti_current", C.c_int64), ("nostop", C.c_int), ("pad", C.c_int),
+                ("sync", C.c_uint8 * 64)]
+
+
+def timestep_gravity(acc, mass, st, prm, eta, dtmax, dtmin=0.0, dtdisp=0.0, timebase=1 << 29, ti_current=0,
+                     bin_old=None, sync=None, pm=None, ids=None, nostop=False):
+    """get_timestep_gravity + the new time bin per particle (timestep.c:284-353, 725-770), TimeMax - TimeBegin = 1.
+    Returns (ti_step, bin, status) with status 0 or the reference's stop code."""
+    acc = np.ascontiguousarray(acc, np.float64)
+    n = len(acc)
+    t = OrTsParams(eta=eta, cf_atime=1.0, cf_a2inv=1.0, cf_hubble_a=1.0, dtmax=dtmax, dtmin=dtmin, dtdisp=dtdisp,
+                   timebase_interval=1.0 / timebase, timebase=timebase, ti_current=ti_current, nostop=int(nostop))
+    for b in range(64):
+        t.sync[b] = 1 if (sync is None or sync[b]) else 0
+    bo = np.zeros(n, np.int8) if bin_old is None else np.ascontiguousarray(bin_old, np.int8)
+    ti = np.zeros(n, np.int64)
+    bn = np.zeros(n, np.int8)
+    pmv = None if pm is None else np.ascontiguousarray(pm, np.float64)
+    idv = None if ids is None else np.ascontiguousarray(ids, np.uint64)
+    s = lib().or_timestep_gravity(n, _ptr(acc), _ptr(pmv), _ptr(np.ascontiguousarray(mass, np.float64)), _ptr(idv),
+                                  _ptr(np.ascontiguousarray(st, np.uint8)), C.byref(prm), C.byref(t), _ptr(bo), _ptr(ti),
+                                  _ptr(bn))
+    return ti, bn, s
+
+
 def shortrange_table(rcut_cells: float = 4.5):
     f = np.zeros(NTAB + 1, np.float32)
     p = np.zeros(NTAB + 1, np.float32)
@@ -424,6 +454,9 @@ def read_output(path):
     r["top"] = np.frombuffer(out["topnodes"], TOPNODE_DTYPE).copy()
     if "order_end" in out:
         r["order_end"] = np.frombuffer(out["order_end"], np.int64)
+    if "tistep" in out:
+        r["tistep"] = np.frombuffer(out["tistep"], np.int64)
+        r["tbin"] = np.frombuffer(out["tbin"], np.int32)
     if "tree_meta" in out:
         meta = np.frombuffer(out["tree_meta"], np.int64)
         r["tree_meta"] = dict(max_part=int(meta[0]), max_nodes=int(meta[1]), num_nodes=int(meta[2]),
@@ -452,8 +485,9 @@ def read_output(path):
 def run_ref(pos, mass, st, periodic, *, box=1.0, asmth=None, rcut=None, theta=0.7, erracc=0.0025,
             softening=(0.01, 0.01), mdom=8, tnf=2.5, passes=2, dump=1, gt=1, first=0, count=None, stride=1,
             timeout=3600, ewald=False, ewald_table_out=None, mns=False, gpu=0, active=1, displace=0.0, minangle=False,
-            direct=0):
-    """Run the compiled reference harness; returns the parsed dump.  ewald=True: the periodic
+            direct=0, tstep=None):
+    """Run the compiled reference harness; returns the parsed dump.  tstep: dict(eta=, dtmax=, dtmin=,
+    dtdisp=) runs the time-step criterion on the final accelerations (TimeMax = 1, Ti_Current = 0).  ewald=True: the periodic
     pure-tree build (no PM, Ewald correction); its table file is cached in oracle/_ref/ewald_cache
     (the reference writes it to the working directory), ewald_table_out dumps the scaled table.
     gpu=1|2: the harness build whose gravity() step goes through the library's C binding
@@ -482,6 +516,8 @@ def run_ref(pos, mass, st, periodic, *, box=1.0, asmth=None, rcut=None, theta=0.
         args = [exe, fin, fout, f"box={box!r}", f"theta={theta!r}", f"erracc={erracc!r}", f"eps0={eps[0]!r}",
                 f"eps1={eps[1]!r}", f"mdom={mdom}", f"tnf={tnf!r}", f"passes={passes}", f"dump={dump}", f"gt={gt}",
                 f"first={first}", f"stride={stride}", f"gpu={gpu}", f"active={active}", f"displace={displace!r}", f"direct={direct}"]
+        if tstep:
+            args += ["tstep=1"] + [f"{k}={v!r}" for k, v in tstep.items()]
         if count is not None:
             args.append(f"count={count}")
         if periodic and not ewald:

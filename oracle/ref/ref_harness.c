@@ -37,7 +37,9 @@
  *             replaces construct_forcetree + gravity_tree by the library's FP64 or FP32 walk through
  *             gpu_gravity.c, the binding AREPO would use), direct (1 = gravity_direct, the
  *             direct summation gravity() runs below DIRECT_SUMMATION_THRESHOLD active particles,
- *             instead of the tree; builds with ALLOW_DIRECT_SUMMATION)
+ *             instead of the tree; builds with ALLOW_DIRECT_SUMMATION), tstep (1 = after the passes,
+ *             get_timestep_gravity and the new gravity time bin of every particle, with eta
+ *             (ErrTolIntAccuracy), dtmax, dtmin, dtdisp (DtDisplacement) and TimeMax = 1)
  */
 #include <math.h>
 #include <stdint.h>
@@ -290,6 +292,7 @@ int main(int argc, char **argv)
   double displace = arg_d(argc, argv, "displace", 0.0);
   int use_gpu     = (int)arg_d(argc, argv, "gpu", 0);
   int use_direct  = (int)arg_d(argc, argv, "direct", 0);
+  int use_tstep   = (int)arg_d(argc, argv, "tstep", 0);
 #ifndef ALLOW_DIRECT_SUMMATION
   if(use_direct)
     {
@@ -582,6 +585,37 @@ int main(int argc, char **argv)
       wr(fo, tv, 8, 6);
       printf("pass=%d N=%d domain=%.6f build=%.6f walk=%.6f (targets=%d, interactions=%lld) gravity_tree=%.6f\n", pass, n,
              t_domain, t_build, t_walk, nt, nint, t_gt);
+    }
+
+  if(use_tstep)
+    {
+      /* the time-step criterion on the final accelerations (time_integration/timestep.c:284-353, 725-770) */
+      All.ErrTolIntAccuracy = arg_d(argc, argv, "eta", 0.025);
+      All.cf_atime = All.cf_a2inv = All.cf_hubble_a = 1.0;
+      All.MaxSizeTimestep   = arg_d(argc, argv, "dtmax", 0.01);
+      All.MinSizeTimestep   = arg_d(argc, argv, "dtmin", 0.0);
+      All.DtDisplacement    = arg_d(argc, argv, "dtdisp", 1.0e30);
+      All.TimeBegin         = 0.0;
+      All.TimeMax           = 1.0;
+      All.Timebase_interval = (All.TimeMax - All.TimeBegin) / TIMEBASE;
+      All.Ti_Current        = 0;
+      wsec(fo, "tistep", (int64_t)n * 8);
+      int64_t *tis = malloc(sizeof(int64_t) * n);
+      int32_t *tbs = malloc(sizeof(int32_t) * n);
+      for(int i = 0; i < n; i++)
+        {
+          integertime ti = get_timestep_gravity(i);
+          int bin        = 0;
+          timebins_get_bin_and_do_validity_checks(ti, &bin, P[i].TimeBinGrav);
+          tis[i] = (int64_t)ti;
+          tbs[i] = bin;
+        }
+      wr(fo, tis, 8, n);
+      wsec(fo, "tbin", (int64_t)n * 4);
+      wr(fo, tbs, 4, n);
+      free(tis);
+      free(tbs);
+      printf("tstep timebase=%lld\n", (long long)TIMEBASE);
     }
 
   /* particle order after the passes (a -3 recovery redoes the domain decomposition) */
