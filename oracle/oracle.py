@@ -454,6 +454,9 @@ def read_output(path):
     r["top"] = np.frombuffer(out["topnodes"], TOPNODE_DTYPE).copy()
     if "order_end" in out:
         r["order_end"] = np.frombuffer(out["order_end"], np.int64)
+    if "gravpm" in out:
+        r["gravpm"] = np.frombuffer(out["gravpm"], np.float64).reshape(-1, 3)
+        r["pmpot"] = np.frombuffer(out["pmpot"], np.float64) if "pmpot" in out else None
     if "tistep" in out:
         r["tistep"] = np.frombuffer(out["tistep"], np.int64)
         r["tbin"] = np.frombuffer(out["tbin"], np.int32)
@@ -485,7 +488,7 @@ def read_output(path):
 def run_ref(pos, mass, st, periodic, *, box=1.0, asmth=None, rcut=None, theta=0.7, erracc=0.0025,
             softening=(0.01, 0.01), mdom=8, tnf=2.5, passes=2, dump=1, gt=1, first=0, count=None, stride=1,
             timeout=3600, ewald=False, ewald_table_out=None, mns=False, gpu=0, active=1, displace=0.0, minangle=False,
-            direct=0, tstep=None):
+            direct=0, tstep=None, pm=False):
     """Run the compiled reference harness; returns the parsed dump.  tstep: dict(eta=, dtmax=, dtmin=,
     dtdisp=) runs the time-step criterion on the final accelerations (TimeMax = 1, Ti_Current = 0).  ewald=True: the periodic
     pure-tree build (no PM, Ewald correction); its table file is cached in oracle/_ref/ewald_cache
@@ -499,6 +502,7 @@ def run_ref(pos, mass, st, periodic, *, box=1.0, asmth=None, rcut=None, theta=0.
         raise ValueError("the MULTIPLE_NODE_SOFTENING harness is a periodic TreePM build")
     exe = os.path.join(REF_DIR, "ref_harness_ewald" if ewald else
                        ("ref_harness_pm_mns" if mns else ("ref_harness_pm_mina" if minangle else
+                                                          "ref_harness_pmfft" if pm else
                                                            ("ref_harness_pm" if periodic else "ref_harness_iso"))))
     if gpu:
         exe += "_gpu"
@@ -518,6 +522,8 @@ def run_ref(pos, mass, st, periodic, *, box=1.0, asmth=None, rcut=None, theta=0.
                 f"first={first}", f"stride={stride}", f"gpu={gpu}", f"active={active}", f"displace={displace!r}", f"direct={direct}"]
         if tstep:
             args += ["tstep=1"] + [f"{k}={v!r}" for k, v in tstep.items()]
+        if pm:
+            args += ["pm=1"]
         if count is not None:
             args.append(f"count={count}")
         if periodic and not ewald:

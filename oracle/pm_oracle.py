@@ -4,10 +4,12 @@ analytic long-range force it approximates.
 
 Only ``tests/`` import this module; the library under ``arepo_b200/`` never does.
 
-Parity status: parity unpinned against the reference -- its PM path needs FFTW, which is not in
-this image, so it cannot be compiled here, and it has no golden vectors. ``pm_periodic`` restates
-its steps (cited per step) in float64 numpy and is pinned to physics instead: ``longrange_ewald`` is the reciprocal-space Ewald sum with the same Gaussian
-split (alpha = 1 / (2 Asmth), the long-range half of the erfc kernel of the tree walk,
+Parity status: pinned to the reference.  FFTW is not in this image, but the reference's own
+pm_periodic.c compiles into a harness build (oracle/ref, config_pmfft.h) whose few FFTW calls are
+served by oracle/ref/fftw_shim.c (a radix-2 FFT); ``pm_periodic`` agrees with that build's
+pmforce_periodic to ~1e-15 of the RMS force (tests/test_pm_oracle.py).  It is also checked against
+physics: ``longrange_ewald`` is the reciprocal-space Ewald sum with the same Gaussian split
+(alpha = 1 / (2 Asmth), the long-range half of the erfc kernel of the tree walk,
 src/gravity/forcetree_walk.c:72-85), evaluated exactly by summing over wave vectors.
 """
 from __future__ import annotations

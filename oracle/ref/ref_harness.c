@@ -39,7 +39,9 @@
  *             direct summation gravity() runs below DIRECT_SUMMATION_THRESHOLD active particles,
  *             instead of the tree; builds with ALLOW_DIRECT_SUMMATION), tstep (1 = after the passes,
  *             get_timestep_gravity and the new gravity time bin of every particle, with eta
- *             (ErrTolIntAccuracy), dtmax, dtmin, dtdisp (DtDisplacement) and TimeMax = 1)
+ *             (ErrTolIntAccuracy), dtmax, dtmin, dtdisp (DtDisplacement) and TimeMax = 1), pm (builds
+ *             with the reference's periodic PM, ref_harness_pmfft: 1 = after the passes,
+ *             pm_init_periodic + pmforce_periodic(0, NULL), dumping GravPM and PM_Potential)
  */
 #include <math.h>
 #include <stdint.h>
@@ -293,6 +295,14 @@ int main(int argc, char **argv)
   int use_gpu     = (int)arg_d(argc, argv, "gpu", 0);
   int use_direct  = (int)arg_d(argc, argv, "direct", 0);
   int use_tstep   = (int)arg_d(argc, argv, "tstep", 0);
+  int use_pm      = (int)arg_d(argc, argv, "pm", 0);
+#ifndef HARNESS_PM
+  if(use_pm)
+    {
+      fprintf(stderr, "ref_harness: pm=1 needs the build with the periodic PM (ref_harness_pmfft)\n");
+      return 1;
+    }
+#endif
 #ifndef ALLOW_DIRECT_SUMMATION
   if(use_direct)
     {
@@ -586,6 +596,43 @@ int main(int argc, char **argv)
       printf("pass=%d N=%d domain=%.6f build=%.6f walk=%.6f (targets=%d, interactions=%lld) gravity_tree=%.6f\n", pass, n,
              t_domain, t_build, t_walk, nt, nint, t_gt);
     }
+
+#ifdef HARNESS_PM
+  if(use_pm)
+    {
+      /* the reference's long-range force on the same particles (gravity/pm/pm_periodic.c:172-248, 1572-1936) */
+      const double asmth = All.Asmth[0], rcut = All.Rcut[0];
+      pm_init_periodic(); /* sets Asmth/Rcut from ASMTH and PMGRID */
+      for(int i = 0; i < n; i++)
+        {
+          for(int k = 0; k < 3; k++)
+            P[i].GravPM[k] = 0;
+#ifdef EVALPOTENTIAL
+          P[i].PM_Potential = 0;
+#endif
+        }
+      double tp0 = wall();
+      pmforce_periodic(0, NULL);
+      double tpm = wall() - tp0;
+      wsec(fo, "gravpm", (int64_t)n * 24);
+      for(int i = 0; i < n; i++)
+        {
+          double g[3] = {P[i].GravPM[0], P[i].GravPM[1], P[i].GravPM[2]};
+          wr(fo, g, 8, 3);
+        }
+#ifdef EVALPOTENTIAL
+      wsec(fo, "pmpot", (int64_t)n * 8);
+      for(int i = 0; i < n; i++)
+        {
+          double v = P[i].PM_Potential;
+          wr(fo, &v, 8, 1);
+        }
+#endif
+      printf("pm asmth=%.17g pm_time=%.6f\n", All.Asmth[0], tpm);
+      All.Asmth[0] = asmth;
+      All.Rcut[0]  = rcut;
+    }
+#endif
 
   if(use_tstep)
     {

@@ -38,8 +38,10 @@ UNUSED_FN(mpz_sgn)
 UNUSED_FN(mpz_sub)
 UNUSED_FN(mpz_tdiv_q_2exp)
 UNUSED_FN(output_compile_time_options)
+#ifndef HAVE_PM_PERIODIC /* the pmfft harness build links the reference's own periodic PM */
 UNUSED_FN(pm_init_periodic)
 UNUSED_FN(pmforce_periodic)
+#endif
 UNUSED_FN(write_only_delaunay_triangulation)
 
 /* endrun() is defined next to main() in the reference; the harness has its own main */
