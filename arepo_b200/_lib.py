@@ -193,6 +193,7 @@ _SIGS = {
     "gpugrav_timestep_gravity": (C.c_int32, [_P, _P, C.c_int64, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_active_particles": (C.c_int32, [_P, C.c_int64, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_set_target_slice": (C.c_int32, [_P, C.c_int32, C.c_int32]),
+    "gpugrav_set_target_slice_cost": (C.c_int32, [_P, C.c_int32, C.c_int32, C.c_int64, _P, C.c_int32]),
     "gpugrav_pm_periodic": (C.c_int32, [_P, C.c_int32, C.c_int64, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_set_ewald_table": (C.c_int32, [_P, C.c_int32, _P, _P, _P, _P]),
     "gpugrav_export_mass_per_type": (C.c_int32, [_P, _P]),

@@ -351,7 +351,8 @@ int32_t gpugrav_destroy(gpugrav_ctx *c)
                         &c->nint_s, &c->oldacc_s, &c->oldacc_in, &c->out_acc, &c->out_pot, &c->out_nint, &c->scratch,
                         &c->g_groups, &c->g_ngroups, &c->g_gpd, &c->g_gseg, &c->g_gflag, &c->g_gid, &c->m_sys, &c->m_doms,
                         &c->pm_pos, &c->pm_mass, &c->pm_acc, &c->pm_pot, &c->ewd, &c->ewd32, &c->n_mpt, &c->w_mpt,
-                        &c->g_mpt, &c->iperm, &c->t_in, &c->t_pos, &c->t_pos_alt, &c->t_idx, &c->t_idx_alt};
+                        &c->g_mpt, &c->iperm, &c->t_in, &c->t_pos, &c->t_pos_alt, &c->t_idx, &c->t_idx_alt,
+                        &c->cost_in, &c->cost_u, &c->cost_p, &c->slice_rng};
   gg::pm_release(c);
   for(auto *b : bufs)
     b->release();
@@ -605,14 +606,39 @@ int32_t gpugrav_set_ewald_table(gpugrav_ctx *c, int32_t en, const double *fx, co
   return GPUGRAV_OK;
 }
 
+int32_t gpugrav_set_target_slice_cost(gpugrav_ctx *c, int32_t slice, int32_t nslices, int64_t n, const float *cost, int32_t mem)
+{
+  if(!c)
+    return GPUGRAV_ERR_INVALID;
+  if(nslices < 1 || slice < 0 || slice >= nslices || (cost && n < 1) || (mem != GPUGRAV_MEM_HOST && mem != GPUGRAV_MEM_DEVICE))
+    return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_set_target_slice_cost: need 0 <= slice < nslices and n >= 1");
+  c->slice    = slice;
+  c->nslices  = nslices;
+  c->cost_set = false;
+  if(!cost)
+    return GPUGRAV_OK;
+  DeviceGuard g(c->device);
+  if(c->cost_in.ensure(n * sizeof(float) + 16) != cudaSuccess)
+    return fail(c, GPUGRAV_ERR_OOM, "gpugrav_set_target_slice_cost: device allocation");
+  CK(cudaMemcpyAsync(c->cost_in.p, cost, n * sizeof(float),
+                     mem == GPUGRAV_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, c->stream),
+     "upload costs");
+  if(mem == GPUGRAV_MEM_HOST)
+    CK(cudaStreamSynchronize(c->stream), "upload costs");  // the caller may reuse its array
+  c->cost_n   = n;
+  c->cost_set = true;
+  return GPUGRAV_OK;
+}
+
 int32_t gpugrav_set_target_slice(gpugrav_ctx *c, int32_t slice, int32_t nslices)
 {
   if(!c)
     return GPUGRAV_ERR_INVALID;
   if(nslices < 1 || slice < 0 || slice >= nslices)
     return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_set_target_slice: need 0 <= slice < nslices");
-  c->slice   = slice;
-  c->nslices = nslices;
+  c->slice    = slice;
+  c->nslices  = nslices;
+  c->cost_set = false;  // equal shares of the targets
   return GPUGRAV_OK;
 }
 
@@ -630,6 +656,8 @@ int walk_impl(gpugrav_ctx *c, int64_t nt, const int32_t *targets, const float *o
   if(!c->built)
     return fail(c, GPUGRAV_ERR_STATE, "gpugrav_walk before gpugrav_build");
   const bool active = targets != nullptr;
+  if(!active && c->cost_set && c->nslices > 1 && c->cost_n != c->n)
+    return fail(c, GPUGRAV_ERR_STATE, "gpugrav_walk: slice costs were set for another particle count");
   if((!acc && !(active && nt == 0)) || (mem != GPUGRAV_MEM_HOST && mem != GPUGRAV_MEM_DEVICE))
     return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_walk: acc must be non-null");
   if(active && (nt < 0 || nt > c->n))
@@ -720,6 +748,9 @@ int walk_impl(gpugrav_ctx *c, int64_t nt, const int32_t *targets, const float *o
               c->groups_active = false;
             }
         }
+      c->slice_rng_on = false;
+      if(!active && we == cudaSuccess)
+        we = gg::slice_cost_stage(c, true);  // cost-balanced slice range, if costs are set
       if(active)
         {
           c->w_tlist    = c->t_pos_alt.as<int32_t>();
@@ -730,12 +761,16 @@ int walk_impl(gpugrav_ctx *c, int64_t nt, const int32_t *targets, const float *o
     }
   else
     {
+      c->slice_rng_on = false;
       if(active)
         {
           c->w_tlist    = c->t_pos_alt.as<int32_t>();
           c->w_ntargets = nt;
         }
-      we = gg::walk64_stage(c, wc);
+      else
+        we = gg::slice_cost_stage(c, false);
+      if(we == cudaSuccess)
+        we = gg::walk64_stage(c, wc);
     }
   c->w_tlist    = nullptr;
   c->w_ntargets = 0;

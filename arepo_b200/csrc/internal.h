@@ -217,6 +217,12 @@ struct gpugrav_ctx
   // (t_pos_alt) and their places in the caller's list (t_idx_alt); w_tlist is null for a walk of every particle
   gg::DevBuf iperm, t_in, t_pos, t_pos_alt, t_idx, t_idx_alt;
   const int32_t *w_tlist = nullptr;
+  // cost-balanced slices (gpugrav_set_target_slice_cost): per-particle cost in caller order, per-unit
+  // costs and their prefix sums, the slice range computed on the device
+  gg::DevBuf cost_in, cost_u, cost_p, slice_rng;
+  bool cost_set     = false;
+  int64_t cost_n    = 0;
+  bool slice_rng_on = false;
   int64_t w_ntargets     = 0;
   bool groups_active     = false;  // the FP32 group table describes an active list, not every particle
   // Ewald correction tables (ewald.cu): FP64 and float4 copies, scaled to ewd_box (or the caller's)
@@ -268,6 +274,7 @@ cudaError_t targets_stage(gpugrav_ctx *c, int64_t nt, const int32_t *d_targets, 
 cudaError_t groups_active_stage(gpugrav_ctx *c, int64_t nt, int cap);
 cudaError_t targets_scatter(gpugrav_ctx *c, int64_t nt, int64_t a, int64_t b, double *acc, double *pot, int32_t *nint);
 cudaError_t slice_mask_stage(gpugrav_ctx *c, bool fp32);
+cudaError_t slice_cost_stage(gpugrav_ctx *c, bool fp32);
 const std::vector<double> &ewald_unit_table();
 cudaError_t ewald_upload(gpugrav_ctx *c, const double *user);
 cudaError_t ewald_ensure(gpugrav_ctx *c);

@@ -612,6 +612,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS
                                                         const uint8_t *__restrict__ tst, const float *__restrict__ oldacc,
                                                         const int *__restrict__ ngroups_dev, const int4 *__restrict__ groups,
                                                         const int32_t *__restrict__ tlist, int slice, int nslices,
+                                                        const int64_t *__restrict__ slice_rng,
                                                         const W32Const *__restrict__ wcp,
                                                         int *__restrict__ stack_base, int *__restrict__ work,
                                                         double *__restrict__ acc_out, double *__restrict__ pot_out,
@@ -637,7 +638,9 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS
   unsigned long long my_total = 0;
   // groups of this target slice; the count lives on the device (no host round trip, graph replays)
   const int64_t ng       = *ngroups_dev;
-  const int g_begin      = (int)(ng * slice / nslices), g_end = (int)(ng * (slice + 1) / nslices);
+  // (or the cost-balanced range computed on the device, slice_rng[0..1])
+  const int g_begin = slice_rng ? (int)slice_rng[0] : (int)(ng * slice / nslices);
+  const int g_end   = slice_rng ? (int)slice_rng[1] : (int)(ng * (slice + 1) / nslices);
 
   while(true)
     {
@@ -1044,10 +1047,16 @@ __global__ void k_grp_fill(int64_t n, const int32_t *__restrict__ flag, const in
 // outputs (sorted order) of the targets outside this slice set to zero; the slice's target range
 // is [start of group g_begin, start of group g_end) with the FP32 group table, else n*s/ns..
 __global__ void k_slice_mask(int64_t n, int slice, int nslices, const int4 *__restrict__ groups, const int *__restrict__ ngroups,
-                             double *__restrict__ acc, double *__restrict__ pot, int32_t *__restrict__ nint)
+                             const int64_t *__restrict__ slice_rng, double *__restrict__ acc, double *__restrict__ pot,
+                             int32_t *__restrict__ nint)
 {
   int64_t t_begin, t_end;
-  if(groups)
+  if(slice_rng)
+    {
+      t_begin = slice_rng[2];
+      t_end   = slice_rng[3];
+    }
+  else if(groups)
     {
       const int64_t ng = *ngroups;
       const int64_t gb = ng * slice / nslices, ge = ng * (slice + 1) / nslices;
@@ -1295,10 +1304,114 @@ cudaError_t walk32_launch(gpugrav_ctx *c)
                                               c->g_pm.as<double4>(), c->g_pst.as<uint8_t>(), c->s_pm.as<double4>(),
                                               c->s_st.as<uint8_t>(), c->oldacc_s.as<float>(), c->g_ngroups.as<int>(),
                                               c->g_groups.as<int4>(), c->w_tlist, c->slice, c->nslices,
+                                              c->slice_rng_on ? c->slice_rng.as<int64_t>() : nullptr,
                                               (const W32Const *)c->scratch.p,
                                               c->g_stack.as<int>(), work, c->acc_s.as<double>(), c->pot_s.as<double>(),
                                               c->nint_s.as<int32_t>(), (unsigned long long *)(c->counters.as<int>() + 32), err);
   return cudaGetLastError();
+}
+
+// ---- cost-balanced target slices ----
+// Cost of every walk group (FP32) or target (FP64) in key order, from the caller's per-particle cost
+// (the previous step's interaction counts, as force_assign_cost_values feeds the reference's domain
+// decomposition, src/gravity/forcetree.c:945-1010).
+__global__ void k_unit_cost(int64_t nu, int64_t n, const int4 *__restrict__ groups, const uint32_t *__restrict__ perm,
+                            const float *__restrict__ cost, double *__restrict__ ucost)
+{
+  for(int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < nu; u += (int64_t)gridDim.x * blockDim.x)
+    {
+      if(groups)
+        {
+          const int4 g = groups[u];
+          double s     = 0;
+          for(int k = 0; k < g.y; k++)
+            s += cost[perm[g.x + k]];
+          ucost[u] = s;
+        }
+      else
+        ucost[u] = cost[perm[u]];
+    }
+}
+
+// units [b(s), b(s+1)) with b(s) the first unit whose exclusive cost prefix reaches s/ns of the total
+// (equal unit counts when the total is 0); rng = (first group, end group, first target, end target)
+__global__ void k_slice_bounds(int64_t nu, int64_t n, const int4 *__restrict__ groups, const double *__restrict__ incl, int slice,
+                               int nslices, int64_t *__restrict__ rng)
+{
+  if(blockIdx.x || threadIdx.x)
+    return;
+  const double total = nu > 0 ? incl[nu - 1] : 0.0;
+  int64_t b[2];
+  for(int e = 0; e < 2; e++)
+    {
+      const int s = slice + e;
+      if(s == 0 || nu == 0)
+        b[e] = 0;
+      else if(s == nslices)
+        b[e] = nu;
+      else if(!(total > 0))
+        b[e] = nu * s / nslices;
+      else
+        {
+          const double want = total * s / nslices;
+          int64_t lo = 0, hi = nu;  // first u with exclusive prefix (incl[u-1]) >= want
+          while(lo < hi)
+            {
+              const int64_t mid = (lo + hi) / 2;
+              const double ex   = mid > 0 ? incl[mid - 1] : 0.0;
+              if(ex >= want)
+                hi = mid;
+              else
+                lo = mid + 1;
+            }
+          b[e] = lo;
+        }
+    }
+  if(groups)
+    {
+      rng[0] = b[0];
+      rng[1] = b[1];
+      rng[2] = b[0] < nu ? groups[b[0]].x : n;
+      rng[3] = b[1] < nu ? groups[b[1]].x : n;
+    }
+  else
+    {
+      rng[0] = rng[1] = 0;
+      rng[2] = b[0];
+      rng[3] = b[1];
+    }
+}
+
+// device-side slice range from the caller's costs (gpugrav_set_target_slice_cost); FP32: in walk
+// groups (the group count is read on the host once, here), FP64: in targets
+cudaError_t slice_cost_stage(gpugrav_ctx *c, bool fp32)
+{
+  c->slice_rng_on = false;
+  if(c->nslices <= 1 || !c->cost_set)
+    return cudaSuccess;
+  cudaStream_t st = c->stream;
+  int64_t nu      = c->n;
+  if(fp32)
+    {
+      int ng = 0;
+      GG_TRY(cudaMemcpyAsync(&ng, c->g_ngroups.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+      GG_TRY(cudaStreamSynchronize(st));
+      nu = ng;
+    }
+  GG_TRY(c->slice_rng.ensure(4 * sizeof(int64_t)));
+  GG_TRY(c->cost_u.ensure((nu + 1) * sizeof(double)));
+  GG_TRY(c->cost_p.ensure((nu + 1) * sizeof(double)));
+  const int4 *groups = fp32 ? c->g_groups.as<int4>() : nullptr;
+  k_unit_cost<<<grid_for(nu, 256), 256, 0, st>>>(nu, c->n, groups, c->perm.as<uint32_t>(), c->cost_in.as<float>(),
+                                                 c->cost_u.as<double>());
+  size_t tb = 0;
+  GG_TRY(cub::DeviceScan::InclusiveSum(nullptr, tb, c->cost_u.as<double>(), c->cost_p.as<double>(), (int)nu, st));
+  GG_TRY(c->sort_tmp.ensure(tb));
+  GG_TRY(cub::DeviceScan::InclusiveSum(c->sort_tmp.p, tb, c->cost_u.as<double>(), c->cost_p.as<double>(), (int)nu, st));
+  k_slice_bounds<<<1, 32, 0, st>>>(nu, c->n, groups, c->cost_p.as<double>(), c->slice, c->nslices, c->slice_rng.as<int64_t>());
+  GG_TRY(cudaGetLastError());
+  c->slice_rng_on = true;
+  return cudaSuccess;
 }
 
 // zero the outputs of the targets outside the current target slice (no-op without slicing)
@@ -1307,7 +1420,8 @@ cudaError_t slice_mask_stage(gpugrav_ctx *c, bool fp32)
   if(c->nslices <= 1)
     return cudaSuccess;
   k_slice_mask<<<grid_for(c->n, 256), 256, 0, c->stream>>>(c->n, c->slice, c->nslices, fp32 ? c->g_groups.as<int4>() : nullptr,
-                                                           fp32 ? c->g_ngroups.as<int>() : nullptr, c->acc_s.as<double>(),
+                                                           fp32 ? c->g_ngroups.as<int>() : nullptr,
+                                                           c->slice_rng_on ? c->slice_rng.as<int64_t>() : nullptr, c->acc_s.as<double>(),
                                                            c->want_pot ? c->pot_s.as<double>() : nullptr, c->nint_s.as<int32_t>());
   return cudaGetLastError();
 }

@@ -295,9 +295,18 @@ __global__ void __launch_bounds__(32 * kWarps, 12) k_walk64(const double4 *__res
 
 cudaError_t walk64_stage(gpugrav_ctx *c, const WalkConst &wc)
 {
-  // targets: every particle, or the active list (gpugrav_walk_targets)
-  const int64_t n       = c->w_tlist ? c->w_ntargets : c->n;
-  const int64_t t_begin = n * c->slice / c->nslices, t_end = n * (c->slice + 1) / c->nslices;
+  // targets: every particle, or the active list (gpugrav_walk_targets); the slice's range from the
+  // device when it is balanced by cost
+  const int64_t n = c->w_tlist ? c->w_ntargets : c->n;
+  int64_t t_begin = n * c->slice / c->nslices, t_end = n * (c->slice + 1) / c->nslices;
+  if(c->slice_rng_on && !c->w_tlist)
+    {
+      int64_t rng[4];
+      GG_TRY(cudaMemcpyAsync(rng, c->slice_rng.p, sizeof(rng), cudaMemcpyDeviceToHost, c->stream));
+      GG_TRY(cudaStreamSynchronize(c->stream));
+      t_begin = rng[2];
+      t_end   = rng[3];
+    }
   const int64_t warps   = (t_end - t_begin + 31) / 32;
   const int64_t blocks  = warps > 0 ? (warps + kWarps - 1) / kWarps : 1;
   auto kern = wc.ewald ? (wc.mns ? k_walk64<true, true> : k_walk64<true, false>)

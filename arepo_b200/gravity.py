@@ -93,6 +93,14 @@ class GravityTree:
         are zero (the slices of G ranks sum to the full result)."""
         self._check(self.lib.gpugrav_set_target_slice(self._ctx, slice_, nslices))
 
+    def set_target_slice_cost(self, slice_: int, nslices: int, cost=None, mem: int = L.MEM_HOST):
+        """Key-ordered target slices of equal cost (per-particle cost in caller order, e.g. the previous
+        step's interaction counts); cost None: equal counts."""
+        n = 0 if cost is None else (cost.shape[0] if hasattr(cost, "shape") else len(cost))
+        if cost is not None and mem == L.MEM_HOST:
+            cost = np.ascontiguousarray(cost, np.float32)
+        self._check(self.lib.gpugrav_set_target_slice_cost(self._ctx, slice_, nslices, n, L.ptr(cost), mem))
+
     def set_stream(self, stream_handle: int | None):
         self._check(self.lib.gpugrav_set_stream(self._ctx, C.c_void_p(stream_handle) if stream_handle else None))
 

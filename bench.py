@@ -466,13 +466,16 @@ def sharded_arm(args):
     tree = sg._tree
     stream = torch.cuda.current_stream()
 
-    acc_d, _ = sg.compute(pos_d, mass_d, st_d, None)  # Barnes-Hut pass -> OldAcc
+    acc_d, _, _ = sg.compute(pos_d, mass_d, st_d, None)  # Barnes-Hut pass -> OldAcc
     oldacc_d = torch.linalg.norm(acc_d, dim=1).to(torch.float32)
     prm.err_tol_theta = 0.0
     prm.err_tol_force_acc = args.err_tol_force_acc
     tree.set_params(prm)
+    # slices of equal cost: each step's interaction counts balance the next step's slices
+    cost_d = None
     for _ in range(args.warmup):
-        acc_d, _ = sg.compute(pos_d, mass_d, st_d, oldacc_d)
+        acc_d, _, ni_d = sg.compute(pos_d, mass_d, st_d, oldacc_d, cost_d)
+        cost_d = ni_d.to(torch.float32)
     torch.cuda.synchronize()
 
     def timed(fn):
@@ -492,7 +495,7 @@ def sharded_arm(args):
     walk_ms, inter = [], []
 
     def step():
-        sg.compute(pos_d, mass_d, st_d, oldacc_d)
+        sg.compute(pos_d, mass_d, st_d, oldacc_d, cost_d)
         tm = tree.timings()
         walk_ms.append(tm.walk_ms)
         inter.append(tm.interactions)
@@ -503,8 +506,8 @@ def sharded_arm(args):
     acc_h = torch.empty((hi - lo, 3), dtype=torch.float64).pin_memory()
 
     def step_e2e():
-        a, _ = sg.compute(pos_h.to(dev, non_blocking=True), mass_h.to(dev, non_blocking=True),
-                          st_h.to(dev, non_blocking=True), old_h.to(dev, non_blocking=True))
+        a, _, _ = sg.compute(pos_h.to(dev, non_blocking=True), mass_h.to(dev, non_blocking=True),
+                             st_h.to(dev, non_blocking=True), old_h.to(dev, non_blocking=True), cost_d)
         acc_h.copy_(a, non_blocking=True)
 
     ms_e2e = timed(step_e2e)
@@ -551,29 +554,17 @@ def sharded_arm(args):
 
 
 def our_arm(args):
+    """One GPU, one process (more ranks run sharded_arm)."""
     import torch
 
     from arepo_b200 import _lib as L
     from arepo_b200 import ics
     from arepo_b200.gravity import GravityTree
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world != args.gpus:
-        log(f"warning: --gpus {args.gpus} but WORLD_SIZE={world}")
+    world, rank, local = 1, 0, int(os.environ.get("LOCAL_RANK", "0"))
+    if args.gpus != 1:
+        log(f"warning: --gpus {args.gpus} with one process")
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
 
     prec = L.PREC_FP32 if args.precision == "fp32" else L.PREC_FP64
     lh = args.log2_half
@@ -619,7 +610,6 @@ def our_arm(args):
     # ---- timed: device-resident inputs ----
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     walk_ms, build_ms, domain_ms, sort_ms, inter = [], [], [], [], []
-    barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         start.record(stream)
@@ -633,13 +623,8 @@ def our_arm(args):
             inter.append(tm.interactions)
         end.record(stream)
         torch.cuda.synchronize()
-    barrier()
     ms = start.elapsed_time(end) / args.steps
     launches_per_step = 5 + tm.build_kernel_launches + 3  # extent x2, keys, gather, (sort: CUB) ; build ; walk gather/walk/scatter
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
 
     # ---- timed: host buffers through the C ABI (end to end) ----
     pos_h = torch.from_numpy(ic["pos"]).pin_memory()
@@ -650,19 +635,13 @@ def our_arm(args):
     pot_h = torch.empty(n, dtype=torch.float64).pin_memory()
     ni_h = torch.empty(n, dtype=torch.int32).pin_memory()
     compute(L.ptr(old_h), L.MEM_HOST, pos_h, mass_h, st_h, acc_h, pot_h, ni_h)
-    barrier()
     torch.cuda.synchronize()
     start.record(stream)
     for _ in range(args.steps):
         compute(L.ptr(old_h), L.MEM_HOST, pos_h, mass_h, st_h, acc_h, pot_h, ni_h)
     end.record(stream)
     torch.cuda.synchronize()
-    barrier()
     ms_e2e = start.elapsed_time(end) / args.steps
-    if dist is not None:
-        t = torch.tensor([ms_e2e], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
 
     # ---- PM long-range force of the same particles (PMGRID = 512), device-resident ----
     pm_acc = torch.empty((n, 3), dtype=torch.float64, device=dev)
@@ -774,7 +753,7 @@ def our_arm(args):
         "tree": {"num_nodes": int(info.num_nodes), "max_depth": int(info.max_depth),
                  "topnodes": int(info.num_topnodes)},
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if not args.no_cpu_baseline:
         try:
             model, ncpu = cpu_info()
             d = run_cpu_reference(max(1, ncpu or 1), args.err_tol_force_acc, 2, log2_half=lh)
@@ -788,13 +767,9 @@ def our_arm(args):
     tree.close()
     del pos_d, mass_d, st_d, acc_d, pot_d, ni_d, oldacc_d
     torch.cuda.empty_cache()
-    if rank == 0 and world == 1 and not args.no_serving:
+    if not args.no_serving:
         line["serving"] = serving_leg(args, local)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    print(json.dumps(line), flush=True)
     return 0
 
 

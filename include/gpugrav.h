@@ -220,6 +220,16 @@ int32_t gpugrav_set_target_slice(gpugrav_ctx *ctx, int32_t slice, int32_t nslice
  * doubles in the reference's node order (parity checks). */
 int32_t gpugrav_export_mass_per_type(gpugrav_ctx *ctx, double *out);
 
+/* The same with slices of equal COST instead of equal target counts: cost (n floats in caller order,
+ * e.g. the interaction counts of the previous step, the load measure force_assign_cost_values gives the
+ * reference's domain decomposition, src/gravity/forcetree.c:945-1010) is summed per FP32 walk group or
+ * FP64 target in key order, and slice s gets the units from the first whose cost prefix reaches s/nslices
+ * of the total to the first that reaches (s+1)/nslices.  Every rank must pass the same costs.  NULL cost:
+ * equal counts (gpugrav_set_target_slice).  n must be the particle count of the following walks; the
+ * costs are copied (active-target walks ignore them). */
+int32_t gpugrav_set_target_slice_cost(gpugrav_ctx *ctx, int32_t slice, int32_t nslices, int64_t n, const float *cost,
+                                      int32_t mem);
+
 /* Periodic box without PM (params: periodic = 1, asmth = 0): the walks use the nearest image of
  * every node and particle plus the reference's Ewald correction per interaction
  * (src/gravity/forcetree_walk.c:469-477, forcetree_ewald.c:268-391). The correction tables are those

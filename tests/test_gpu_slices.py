@@ -47,3 +47,38 @@ def test_slices_sum_to_unsliced_walk(name, precision, cuda_lib):
             assert np.all(hit == 1)  # each target walked by exactly one slice
         with pytest.raises(L.GpuGravError):
             t.set_target_slice(3, 3)
+
+
+@pytest.mark.parametrize("precision", [L.PREC_FP32, L.PREC_FP64])
+def test_cost_balanced_slices_sum_to_unsliced_walk(precision, cuda_lib):
+    """Slices of equal cost (the previous walk's interaction counts, as force_assign_cost_values):
+    still every target exactly once and the sum bitwise the unsliced walk; the slices' interaction
+    totals are far more even than with equal target counts on the zoom box."""
+    ic = CASES["zoom"]()
+    prm = ics.params_for(ic, precision=precision)
+    g = 4
+    with GravityTree(prm) as t:
+        t.domain_decomposition(ic["pos"], ic["mass"], ic["softtype"])
+        t.construct_forcetree()
+        a_bh, _, _ = t.gravity_tree()
+        oldacc = np.linalg.norm(a_bh, axis=1).astype(np.float32)
+        prm.err_tol_theta = 0.0
+        t.set_params(prm)
+        full_a, full_p, full_n = t.gravity_tree(oldacc)
+        cost = full_n.astype(np.float32)
+        sa, sp, sn = np.zeros_like(full_a), np.zeros_like(full_p), np.zeros_like(full_n)
+        loads_cost, loads_count = [], []
+        for s in range(g):
+            t.set_target_slice_cost(s, g, cost)
+            a, p, ni = t.gravity_tree(oldacc)
+            sa += a
+            sp += p
+            sn += ni
+            loads_cost.append(int(ni.sum()))
+            t.set_target_slice(s, g)
+            loads_count.append(int(t.gravity_tree(oldacc)[2].sum()))
+        t.set_target_slice(0, 1)
+    assert np.array_equal(sa, full_a) and np.array_equal(sp, full_p) and np.array_equal(sn, full_n)
+    imb_cost = max(loads_cost) / np.mean(loads_cost)
+    imb_count = max(loads_count) / np.mean(loads_count)
+    assert imb_cost < 1.05 and imb_cost < imb_count, (loads_cost, loads_count)
