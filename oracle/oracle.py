@@ -80,9 +80,11 @@ def build_oracle(force: bool = False) -> str:
     return LIB_PATH
 
 
-def build_ref(ref_root: str = "/root/reference") -> bool:
-    """Compile the reference harness when the reference tree is present; returns availability."""
-    if os.path.isdir(os.path.join(ref_root, "src", "gravity")):
+def build_ref(ref_root: str | None = None) -> bool:
+    """Compile the reference harness from the reference tree at ref_root (default: the AREPO_REFERENCE
+    environment variable) when that tree is present; returns availability."""
+    ref_root = ref_root or os.environ.get("AREPO_REFERENCE", "")
+    if ref_root and os.path.isdir(os.path.join(ref_root, "src", "gravity")):
         subprocess.check_call(
             ["make", "-s", "-j8", "-C", os.path.join(HERE, "ref"), f"REF={ref_root}", f"OUT={REF_DIR}"]
         )
