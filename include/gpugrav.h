@@ -47,7 +47,8 @@ typedef enum gpugrav_status
   GPUGRAV_ERR_INVALID     = -10, /* bad argument */
   GPUGRAV_ERR_OOM         = -11, /* device or pinned host allocation failed */
   GPUGRAV_ERR_CUDA        = -12, /* CUDA runtime error; gpugrav_last_error() has the text */
-  GPUGRAV_ERR_TIMEOUT     = -13, /* a bounded device-side wait gave up (serving loop) */
+  GPUGRAV_ERR_TIMEOUT     = -13, /* reserved for a bounded device-side wait that gives up; no entry point of this
+                                    build waits on the device (every wait is a stream synchronisation) */
   GPUGRAV_ERR_STATE       = -14, /* call order violated (e.g. walk before build) */
   GPUGRAV_ERR_DEEP_TREE   = -15, /* tree deeper than the walk's fixed limits (pathological input) */
   GPUGRAV_ERR_UNSUPPORTED = -16, /* option not available in this build */
