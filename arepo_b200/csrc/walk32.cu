@@ -41,9 +41,6 @@ namespace
 constexpr int kWarps   = GG_W32_WARPS;    // warps per block
 constexpr int kEvalAt  = GG_W32_EVAL_AT;  // evaluate once this many entries are queued
 constexpr int kUnroll  = GG_W32_UNROLL;   // list entries in flight per lane in the evaluation loop
-#ifndef GG_W32_PREFETCH
-#define GG_W32_PREFETCH 1  // L1 prefetch of the next node step's records and of opened nodes' particles
-#endif
 #ifndef GG_W32_MINBLOCKS
 #define GG_W32_MINBLOCKS 5  // blocks per SM the register budget is sized for (96 registers a thread)
 #endif
@@ -265,9 +262,6 @@ __device__ __forceinline__ float rsqrt_normal(float x)
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
-
-// L1 prefetch of the 128-byte line holding p (no register result)
-__device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
 __device__ __forceinline__ float rsqrtR(float x) { return rsqrt_normal(x); }
 __device__ __forceinline__ double rsqrtR(double x) { return rsqrt(x); }
@@ -918,11 +912,8 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS
           push<R, PERIODIC>(L, action == 1 && !split, entry, (R)hj, ent_d2, fmaxf(h_grp, hj), ex, ey, ez, w, lt_mask);
           t_next = 0;
           t_end  = __ballot_sync(0xffffffffu, action == 1 && split) ? w.nsoft : 0;
-          // particles of opened nodes: pending rounds (their records prefetched into L1, 4 per line)
+          // particles of opened nodes: pending rounds
           const int npx = (action == 2) ? np : 0;
-          if(GG_W32_PREFETCH)
-            for(int o = 0; o < npx; o += 4)
-              prefetch_l1(g_pm + fp + o);
           pinc          = wscan_incl(npx, lane);
           ptot          = __shfl_sync(0xffffffffu, pinc, 31);
           pexc          = pinc - npx;
@@ -942,20 +933,6 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS
           else if(lane == 0)
             atomicOr(err, 16);  // stack too small: the walk of this group is incomplete
           __syncwarp();
-          if(GG_W32_PREFETCH)
-            {
-              // the next node step takes the top of the stack: bring those node records into L1 now,
-              // so that their loads there hit while this step's particle rounds and any list
-              // evaluation run in between (prefetches take no registers)
-              const int nt = sp < 32 ? sp : 32;
-              if(lane < nt)
-                {
-                  const int nx = stack[sp - nt + lane];
-                  prefetch_l1(g_sm + nx);
-                  prefetch_l1(g_rel + nx);
-                  prefetch_l1(g_kids + nx);
-                }
-            }
         }
 #pragma unroll
       for(int k = 0; k < TPL; k++)
