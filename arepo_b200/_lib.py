@@ -190,6 +190,7 @@ _SIGS = {
     "gpugrav_walk": (C.c_int32, [_P, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_walk_targets": (C.c_int32, [_P, C.c_int64, _P, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_gravity_direct": (C.c_int32, [_P, C.c_int64, _P, _P, _P, _P, _P, C.c_int32]),
+    "gpugrav_direct_split": (C.c_int32, [_P, C.c_int64, _P, _P, _P, _P, _P]),
     "gpugrav_timestep_gravity": (C.c_int32, [_P, _P, C.c_int64, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_active_particles": (C.c_int32, [_P, C.c_int64, _P, _P, _P, _P, C.c_int32]),
     "gpugrav_set_target_slice": (C.c_int32, [_P, C.c_int32, C.c_int32]),

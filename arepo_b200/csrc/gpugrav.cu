@@ -1162,6 +1162,62 @@ int32_t gpugrav_get_timings(gpugrav_ctx *c, gpugrav_timings *t)
   return GPUGRAV_OK;
 }
 
+int32_t gpugrav_direct_split(gpugrav_ctx *c, int64_t ntargets, const int64_t *targets, double *acc_total, double *pot_total,
+                             double *acc_short, double *pot_short)
+{
+  if(!c)
+    return GPUGRAV_ERR_INVALID;
+  const bool treepm = c->prm.periodic && c->prm.asmth > 0;
+  if((acc_short || pot_short) && !treepm)
+    return fail(c, GPUGRAV_ERR_INVALID, "gpugrav_direct_split: the short-range part needs a TreePM context");
+  if(!c->loaded)
+    return fail(c, GPUGRAV_ERR_STATE, "gpugrav_direct_split before gpugrav_load");
+  std::vector<double> a, p;
+  if(acc_short || pot_short)
+    {
+      a.resize(3 * ntargets + 3);
+      p.resize(ntargets + 1);
+      int s = gpugrav_direct(c, ntargets, targets, GPUGRAV_DIRECT_FULL, a.data(), p.data());
+      if(s != GPUGRAV_OK)
+        return s;
+      // the reference adds mass pi / (Asmth^2 V) per source to the short-range potential
+      std::vector<double> m(c->n);
+      CK(cudaMemcpyAsync(m.data(), c->mass_in.p, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "masses");
+      CK(cudaStreamSynchronize(c->stream), "masses");
+      const double box = c->prm.box_size, as = c->prm.asmth;
+      double add = 0;
+      for(int64_t j = 0; j < c->n; j++)
+        add += m[j] * M_PI / (as * as * box * box * box);
+      if(acc_short)
+        memcpy(acc_short, a.data(), 3 * ntargets * sizeof(double));
+      if(pot_short)
+        for(int64_t t = 0; t < ntargets; t++)
+          pot_short[t] = p[t] + add;
+    }
+  if(acc_total || pot_total)
+    {
+      // Newtonian pairs; in a periodic box with the Ewald correction: the direct sum of a context
+      // without the TreePM split
+      a.assign(3 * ntargets + 3, 0.0);
+      p.assign(ntargets + 1, 0.0);
+      const gpugrav_params keep = c->prm;
+      if(treepm)
+        {
+          c->prm.asmth = 0.0;
+          c->prm.rcut  = 0.0;
+        }
+      int s = gpugrav_direct(c, ntargets, targets, GPUGRAV_DIRECT_FULL, a.data(), p.data());
+      c->prm = keep;
+      if(s != GPUGRAV_OK)
+        return s;
+      if(acc_total)
+        memcpy(acc_total, a.data(), 3 * ntargets * sizeof(double));
+      if(pot_total)
+        memcpy(pot_total, p.data(), ntargets * sizeof(double));
+    }
+  return GPUGRAV_OK;
+}
+
 int32_t gpugrav_direct(gpugrav_ctx *c, int64_t ntargets, const int64_t *targets, int32_t mode, double *acc, double *pot)
 {
   if(!c || ntargets < 0 || (ntargets > 0 && (!targets || !acc)) || (mode != GPUGRAV_DIRECT_FULL && mode != GPUGRAV_DIRECT_CUT))

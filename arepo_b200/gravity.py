@@ -271,6 +271,17 @@ class GravityTree:
         self._check(self.lib.gpugrav_get_timings(self._ctx, C.byref(t)))
         return t
 
+    def direct_split(self, targets):
+        """FORCETEST's split (gravtree_forcetest.c:537-620): (acc_total, pot_total, acc_short, pot_short);
+        the short-range part only for TreePM contexts (else None)."""
+        tg = np.ascontiguousarray(targets, np.int64)
+        nt = len(tg)
+        at, pt = np.empty((nt, 3)), np.empty(nt)
+        treepm = bool(self.params.periodic) and self.params.asmth > 0
+        a_s, p_s = (np.empty((nt, 3)), np.empty(nt)) if treepm else (None, None)
+        self._check(self.lib.gpugrav_direct_split(self._ctx, nt, L.ptr(tg), L.ptr(at), L.ptr(pt), L.ptr(a_s), L.ptr(p_s)))
+        return at, pt, a_s, p_s
+
     def direct(self, targets, cut: bool = False) -> tuple[np.ndarray, np.ndarray]:
         """FP64 direct summation for the given caller indices (accuracy instrument). cut=True keeps
         only pairs closer than Rcut (the range the walk evaluates) in a periodic TreePM run."""

@@ -59,10 +59,10 @@ METRIC = "tree-gravity particles/s at N=2^24 (RMS force err ≤1e-3); serving p5
 UNIT = "particles/s"
 FLOPS_PER_INTERACTION = 23.0  # convention of the path's roofline
 # DRAM bytes (read + write) of one FP32 walk launch per particle: ncu capture of the zoom box at
-# N=2^21 (dram__bytes_read.sum + dram__bytes_write.sum = 284.5 MB + 78.4 MB), scaled by the
+# N=2^21 (dram__bytes_read.sum + dram__bytes_write.sum = 285.5 MB + 78.0 MB), scaled by the
 # particle count (the walk reads the tree and the particles once from DRAM; everything else hits
 # in L2)
-WALK32_DRAM_BYTES_PER_PARTICLE = 362.9e6 / (1 << 21)
+WALK32_DRAM_BYTES_PER_PARTICLE = 363.5e6 / (1 << 21)
 # ErrTolForceAcc of the per-target FP64 walk in the precision ablation: the value at which its RMS
 # error on the zoom box matches the FP32 walk's at 5e-5 (8.1e-4 against 9.3e-4)
 ABLATION_FP64_ALPHA = 2e-5
@@ -680,6 +680,20 @@ def our_arm(args):
                      reference="FP64 direct sum over pairs closer than Rcut with the exact erfc factor (the range the "
                                "walk evaluates): the tree approximation error",
                      vs_full_short_range=err_stats(acc_full))
+    # total force (tree short range + PM long range, PMGRID 512) against the Ewald-corrected direct sum of
+    # every pair on 1024 of the targets (FORCETEST's ftrue, gpugrav_direct_split)
+    tg_tot = tg[:: max(1, len(tg) // 1024)][:1024]
+    pm_acc = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    s = lib.gpugrav_pm_periodic(ctx, 512, n, L.ptr(pos_d), L.ptr(mass_d), L.ptr(pm_acc), None, L.MEM_DEVICE)
+    if s != 0:
+        raise L.GpuGravError(s, lib.gpugrav_last_error(ctx).decode())
+    a_true, _, a_short, _ = tree.direct_split(tg_tot)
+    a_treepm = acc_h.numpy()[tg_tot] + pm_acc.cpu().numpy()[tg_tot]
+    del pm_acc
+    acc_stats["total_force"] = dict(err_stats_of(a_treepm, a_true), targets=int(len(tg_tot)),
+                                    reference="tree (FP32 walk) + PM (PMGRID 512) against the Ewald-corrected FP64 direct "
+                                              "sum of every pair (FORCETEST's ftrue)",
+                                    pm_vs_direct_long_range=err_stats_of(a_treepm - acc_h.numpy()[tg_tot], a_true - a_short))
 
     # ---- precision ablation on the same particles and tree code: the FP32 walk's algorithm with FP64
     # arithmetic, and the per-target FP64 walk (the reference's decisions) at matched accuracy ----

@@ -286,6 +286,15 @@ enum
   GPUGRAV_DIRECT_CUT  = 1
 };
 int32_t gpugrav_direct(gpugrav_ctx *ctx, int64_t ntargets, const int64_t *targets, int32_t mode, double *acc, double *pot);
+/* FORCETEST's split (gravity_forcetest_evaluate, src/gravity/gravtree_forcetest.c:537-620) for the given
+ * targets: acc_total/pot_total the correct direct-summation force and potential (spline-softened
+ * Newtonian pairs plus, in a periodic box, the Ewald correction of every pair -- ftrue), and for a
+ * TreePM context acc_short/pot_short the short-range part with the exact erfc factor (fsr, the best the
+ * tree can deliver; the potential with the reference's constant M_total pi / (Asmth^2 V)), so that
+ * ftrue - fsr is the long-range force the PM should deliver.  Any output may be NULL; the short-range
+ * outputs need periodic with asmth > 0. */
+int32_t gpugrav_direct_split(gpugrav_ctx *ctx, int64_t ntargets, const int64_t *targets, double *acc_total, double *pot_total,
+                             double *acc_short, double *pot_short);
 
 /* ---- small-N direct summation (gravity_direct, src/gravity/gravdirect.c:61-257) ----
  * What gravity() runs instead of the tree when fewer than DIRECT_SUMMATION_THRESHOLD particles are
