@@ -456,8 +456,10 @@ __device__ __forceinline__ void near(const V4<R> e, const R hj, Tgt<R> &T, const
 #ifdef GG_WALK32_STATS
 }  // namespace
 // measurement build only: [0] list entries evaluated per lane, [1] node tests, [2] particle candidates,
-// [3] groups, [4] entries inside Rcut of every target, [5] border entries, [6] warp steps
-__device__ unsigned long long g_walk_stats[8];
+// [3] groups, [4] entries inside Rcut of every target, [5] border entries, [6] warp steps, [7] steps
+// with a per-target vote, [8] voting nodes, [9] particle rounds, [10] list evaluations
+constexpr int kWalkStats = 12;
+__device__ unsigned long long g_walk_stats[kWalkStats];
 namespace
 {
 #define WALK_STAT(i, v)                       \
@@ -729,6 +731,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS
           if(flush)
             {
               WALK_STAT(0, queued);
+              WALK_STAT(10, 1);
               evaluate<R, PERIODIC, POT, TPL, EWALD>(L, T, w);
               __syncwarp();
             }
@@ -749,6 +752,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS
               // Rcut of the whole group are dropped
               const int q = q0 + lane;
               q0 += 32;
+              WALK_STAT(9, 1);
               int owner = 0;  // owner lane: number of lanes whose inclusive prefix is <= q
 #pragma unroll
               for(int s = 16; s >= 1; s >>= 1)
@@ -872,8 +876,10 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS
                 }
             }
           // per-target vote: the node stays open only if some target's own criterion opens it
-          if(__ballot_sync(0xffffffffu, vote))
+          if(const unsigned vm = __ballot_sync(0xffffffffu, vote))
             {
+              WALK_STAT(7, 1);
+              WALK_STAT(8, __popc(vm));
               bool need    = false;
               const float L = vrel.w, L2 = L * L;
 #pragma unroll
@@ -1437,9 +1443,9 @@ cudaError_t walk32_stage(gpugrav_ctx *c, const WalkConst &wc)
 // measurement build only: read and reset the walk statistics of the current device
 extern "C" int gpugrav_walk_stats(unsigned long long *out)
 {
-  if(cudaMemcpyFromSymbol(out, gg::g_walk_stats, sizeof(unsigned long long) * 8) != cudaSuccess)
+  if(cudaMemcpyFromSymbol(out, gg::g_walk_stats, sizeof(unsigned long long) * gg::kWalkStats) != cudaSuccess)
     return -1;
-  unsigned long long z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long z[gg::kWalkStats] = {};
   return cudaMemcpyToSymbol(gg::g_walk_stats, z, sizeof(z)) == cudaSuccess ? 0 : -1;
 }
 #endif
