@@ -42,7 +42,7 @@ constexpr int kWarps   = GG_W32_WARPS;    // warps per block
 constexpr int kEvalAt  = GG_W32_EVAL_AT;  // evaluate once this many entries are queued
 constexpr int kUnroll  = GG_W32_UNROLL;   // list entries in flight per lane in the evaluation loop
 #ifndef GG_W32_MINBLOCKS
-#define GG_W32_MINBLOCKS 5  // blocks per SM the register budget is sized for (96 registers a thread)
+#define GG_W32_MINBLOCKS 6  // blocks per SM the register budget is sized for (80 registers a thread, 31 KB of shared memory a block)
 #endif
 // capacity (Cap below): accepted nodes (<= 32) join a list holding fewer than kEvalAt entries;
 // particles are added at most 32 per round and the list is evaluated first whenever a round could
@@ -86,7 +86,7 @@ struct Cap
   static constexpr int eval     = sizeof(R) == 4 ? kEvalAt : 96;
   static constexpr int list     = eval + 64;
   static constexpr int near_at  = sizeof(R) == 4 ? kNearAt : 32;
-  static constexpr int near_cap = near_at + 64;
+  static constexpr int near_cap = near_at + 32;
 };
 template <typename R>
 struct V4T;
@@ -126,15 +126,19 @@ struct W32Const
   int periodic, bh;
   float soft[GPUGRAV_MAX_SOFTTYPES + 1];
   float4 tab[kNtab + 1];  // (f[i], f[i+1] - f[i], p[i], p[i+1] - p[i]): force table times 1/Asmth^2, potential table
-  double rcut2_d, asmthfac_d;  // FP64 walk: Rcut^2 and the table index factor in double
-  double4 tab64[kNtab + 1];    // FP64 walk: the table above in double
   const float4 *ewd;       // Ewald correction (fx, fy, fz, pot) per table entry (pure periodic tree)
   float ewd_fac;           // 2 EN / L
   int mns;                 // MULTIPLE_NODE_SOFTENING: nodes used per softening type
   const float *mpt;        // per-type node masses, breadth-first order, nsoft each
   int nsoft;
   int minangle;            // ACTIVATE_MINIMUM_OPENING_ANGLE
+  // FP64 form only (the FP32 kernels do not copy these into shared memory)
+  double rcut2_d, asmthfac_d;  // Rcut^2 and the table index factor in double
+  double4 tab64[kNtab + 1];    // the table above in double
 };
+// bytes of the constants a kernel of arithmetic type R keeps in shared memory
+template <typename R>
+constexpr int kW32Bytes = sizeof(R) == 4 ? (int)offsetof(W32Const, rcut2_d) : (int)sizeof(W32Const);
 
 // ------------------------------------------------------------------------------
 // layout
@@ -303,8 +307,7 @@ template <typename R>
 struct Tgt
 {
   R x, y, z, h;             // position relative to the group centre, softening
-  R ax, ay, az, pot;        // partial sums of the current list batch
-  double dax, day, daz, dpot;  // batch partials accumulated in FP64
+  R ax, ay, az, pot;        // partial sums of the current list batch (folded into FP64 sums in shared memory)
   int ni;
 };
 
@@ -539,9 +542,10 @@ struct List
   int na, nb, nn;
 };
 
-// Evaluates and empties the list, then folds the batch partials into the FP64 sums.
+// Evaluates and empties the list, then folds the batch partials into the lane's FP64 sums (shared
+// memory, dsum[(4k + c) * 32] for target k and component c = x, y, z, potential).
 template <typename R, bool PERIODIC, bool POT, int TPL, bool EWALD = false>
-__device__ __forceinline__ void evaluate(List<R> &L, Tgt<R> (&T)[TPL], const W32Const &w)
+__device__ __forceinline__ void evaluate(List<R> &L, Tgt<R> (&T)[TPL], double *dsum, const W32Const &w)
 {
   WALK_STAT(4, L.na);
   WALK_STAT(5, L.nb);
@@ -552,10 +556,11 @@ __device__ __forceinline__ void evaluate(List<R> &L, Tgt<R> (&T)[TPL], const W32
   for(int k = 0; k < TPL; k++)
     {
       T[k].ni += L.na;
-      T[k].dax += T[k].ax;
-      T[k].day += T[k].ay;
-      T[k].daz += T[k].az;
-      T[k].dpot += T[k].pot;
+      dsum[(4 * k + 0) * 32] += T[k].ax;
+      dsum[(4 * k + 1) * 32] += T[k].ay;
+      dsum[(4 * k + 2) * 32] += T[k].az;
+      if(POT)
+        dsum[(4 * k + 3) * 32] += T[k].pot;
       T[k].ax = T[k].ay = T[k].az = T[k].pot = R(0);
     }
   L.na = L.nb = L.nn = 0;
@@ -621,12 +626,19 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS
                                                         int32_t *__restrict__ nint_out, unsigned long long *__restrict__ total,
                                                         int *__restrict__ err)
 {
-  __shared__ W32Const w;
+  __shared__ __align__(16) unsigned char w_raw[kW32Bytes<R>];
+  const W32Const &w = *reinterpret_cast<const W32Const *>(w_raw);
   __shared__ V4<R> il_p[kWarps][Cap<R>::list];
   __shared__ V4<R> il_np[kWarps][Cap<R>::near_cap];
   __shared__ R il_nh[kWarps][Cap<R>::near_cap];
-  for(int t = threadIdx.x; t < (int)(sizeof(W32Const) / 4); t += blockDim.x)
-    ((int *)&w)[t] = ((const int *)wcp)[t];
+  // cold per-lane and per-warp state kept out of registers: the FP64 sums of the lanes' targets,
+  // ErrTolForceAcc x |OldAcc| of the targets (read by the per-target vote), the warp's interaction total
+  __shared__ double dsum_sh[kWarps][4 * TPL][32];
+  __shared__ float aold_sh[kWarps][32 * TPL];
+  __shared__ unsigned long long total_sh[kWarps];
+  static_assert(kW32Bytes<R> % 4 == 0, "constants copied in 4-byte words");
+  for(int t = threadIdx.x; t < kW32Bytes<R> / 4; t += blockDim.x)
+    ((int *)w_raw)[t] = ((const int *)wcp)[t];
   __syncthreads();
 
   const int warp         = threadIdx.x >> 5;
@@ -637,7 +649,9 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS
   L.P  = il_p[warp];
   L.NP = il_np[warp];
   L.NH = il_nh[warp];
-  unsigned long long my_total = 0;
+  double *dsum = &dsum_sh[warp][0][lane];
+  if(lane == 0)
+    total_sh[warp] = 0;
   // groups of this target slice; the count lives on the device (no host round trip, graph replays)
   const int64_t ng       = *ngroups_dev;
   // (or the cost-balanced range computed on the device, slice_rng[0..1])
@@ -662,7 +676,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS
       WALK_STAT(3, 1);
       double4 p[TPL];
       double mnx = 1e300, mxx = -1e300, mny = 1e300, mxy = -1e300, mnz = 1e300, mxz = -1e300;
-      float hmin_l = 3.0e38f, hmax_l = 0.0f, amin_l = 3.0e38f, a_l[TPL];
+      float hmin_l = 3.0e38f, hmax_l = 0.0f, amin_l = 3.0e38f;
 #pragma unroll
       for(int k = 0; k < TPL; k++)
         {
@@ -671,13 +685,14 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS
           // consecutive entries of the active list
           const int64_t tt = tlist ? (int64_t)tlist[t0 + (s < cnt ? s : 0)] : t0 + (s < cnt ? s : 0);
           p[k]             = tpm[tt];
-          a_l[k]           = w.erracc * oldacc[tt];
+          const float a_l  = w.erracc * oldacc[tt];
+          aold_sh[warp][s] = a_l;
           mnx = fmin(mnx, p[k].x), mxx = fmax(mxx, p[k].x);
           mny = fmin(mny, p[k].y), mxy = fmax(mxy, p[k].y);
           mnz = fmin(mnz, p[k].z), mxz = fmax(mxz, p[k].z);
           hmin_l = fminf(hmin_l, w.soft[tst[tt]]);
           hmax_l = fmaxf(hmax_l, w.soft[tst[tt]]);
-          amin_l = fminf(amin_l, a_l[k]);
+          amin_l = fminf(amin_l, a_l);
         }
       // group box (FP64), centre g, half extent (rounded up)
       mnx = wmin(mnx), mxx = wmax(mxx), mny = wmin(mny), mxy = wmax(mxy), mnz = wmin(mnz), mxz = wmax(mxz);
@@ -700,7 +715,9 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS
           const int sk = lane + 32 * k < cnt ? lane + 32 * k : 0;
           T[k].h       = (R)w.soft[tst[tlist ? (int64_t)tlist[t0 + sk] : t0 + sk]];
           T[k].ax = T[k].ay = T[k].az = T[k].pot = R(0);
-          T[k].dax = T[k].day = T[k].daz = T[k].dpot = 0.0;
+#pragma unroll
+          for(int c = 0; c < 4; c++)
+            dsum[(4 * k + c) * 32] = 0.0;
           T[k].ni = 0;
         }
 
@@ -732,7 +749,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS
             {
               WALK_STAT(0, queued);
               WALK_STAT(10, 1);
-              evaluate<R, PERIODIC, POT, TPL, EWALD>(L, T, w);
+              evaluate<R, PERIODIC, POT, TPL, EWALD>(L, T, dsum, w);
               __syncwarp();
             }
           if(t_next < t_end)
@@ -888,7 +905,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS
                   {
                     const float tx = (float)__shfl_sync(0xffffffffu, T[k].x, i), ty = (float)__shfl_sync(0xffffffffu, T[k].y, i),
                                 tz = (float)__shfl_sync(0xffffffffu, T[k].z, i), th = (float)__shfl_sync(0xffffffffu, T[k].h, i),
-                                ta = __shfl_sync(0xffffffffu, a_l[k], i);
+                                ta = aold_sh[warp][i + 32 * k];
                     if(vote && !need && i + 32 * k < cnt)
                       {
                         const float enx = (float)entry.x, eny = (float)entry.y, enz = (float)entry.z;
@@ -947,20 +964,27 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS
           if(s < cnt)
             {
               const int64_t t    = tlist ? (int64_t)tlist[t0 + s] : t0 + s;
-              acc_out[3 * t + 0] = T[k].dax;
-              acc_out[3 * t + 1] = T[k].day;
-              acc_out[3 * t + 2] = T[k].daz;
+              acc_out[3 * t + 0] = dsum[(4 * k + 0) * 32];
+              acc_out[3 * t + 1] = dsum[(4 * k + 1) * 32];
+              acc_out[3 * t + 2] = dsum[(4 * k + 2) * 32];
               if(POT)
-                pot_out[t] = T[k].dpot;
+                pot_out[t] = dsum[(4 * k + 3) * 32];
               nint_out[t] = T[k].ni;
-              my_total += (unsigned long long)T[k].ni;
             }
         }
+      // the group's interactions (idle slots count none)
+      unsigned long long gtot = 0;
+#pragma unroll
+      for(int k = 0; k < TPL; k++)
+        gtot += lane + 32 * k < cnt ? (unsigned long long)T[k].ni : 0ull;
+      for(int o = 16; o > 0; o >>= 1)
+        gtot += __shfl_xor_sync(0xffffffffu, gtot, o);
+      if(lane == 0)
+        total_sh[warp] += gtot;
+      __syncwarp();
     }
-  for(int o = 16; o > 0; o >>= 1)
-    my_total += __shfl_xor_sync(0xffffffffu, my_total, o);
-  if(lane == 0 && my_total)
-    atomicAdd(total, my_total);
+  if(lane == 0 && total_sh[warp])
+    atomicAdd(total, total_sh[warp]);
 }
 
 // ---- walk groups -------------------------------------------------------------------------
