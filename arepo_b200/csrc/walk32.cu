@@ -40,10 +40,19 @@ namespace
 #endif
 constexpr int kWarps   = GG_W32_WARPS;    // warps per block
 constexpr int kEvalAt  = GG_W32_EVAL_AT;  // evaluate once this many entries are queued
-constexpr int kUnroll  = GG_W32_UNROLL;   // list entries in flight per lane in the evaluation loop
 #ifndef GG_W32_MINBLOCKS
 #define GG_W32_MINBLOCKS 6  // blocks per SM the register budget is sized for (80 registers a thread, 31 KB of shared memory a block)
 #endif
+// two targets per lane: fewer entries in flight, 96 registers (5 blocks per SM)
+#ifndef GG_W32_UNROLL2
+#define GG_W32_UNROLL2 4
+#endif
+#ifndef GG_W32_MINBLOCKS2
+#define GG_W32_MINBLOCKS2 5
+#endif
+// list entries in flight per lane in the evaluation loop
+template <int TPL>
+constexpr int kUnroll = TPL == 2 ? GG_W32_UNROLL2 : GG_W32_UNROLL;
 // capacity (Cap below): accepted nodes (<= 32) join a list holding fewer than kEvalAt entries;
 // particles are added at most 32 per round and the list is evaluated first whenever a round could
 // overflow it.  Entries inside some target's softening length go to a separate, smaller near list,
@@ -489,26 +498,27 @@ __device__ __forceinline__ void evaluate_region(const V4<R> *__restrict__ LP, co
                                                 const W32Const &w)
 {
   int j = 0;
-  for(; j + kUnroll <= nl; j += kUnroll)
+  constexpr int U = kUnroll<TPL>;
+  for(; j + U <= nl; j += U)
     {
-      V4<R> e[kUnroll];
-      R hj[kUnroll];
+      V4<R> e[U];
+      R hj[U];
 #pragma unroll
-      for(int u = 0; u < kUnroll; u++)
+      for(int u = 0; u < U; u++)
         {
           e[u]  = LP[j + u];
           hj[u] = CHECK ? LH[j + u] : R(0);
         }
       bool soft = false;
 #pragma unroll
-      for(int u = 0; u < kUnroll; u++)
+      for(int u = 0; u < U; u++)
 #pragma unroll
         for(int k = 0; k < TPL; k++)
           soft |= far<R, PERIODIC, POT, EWALD, CHECK, MASK>(e[u], hj[u], T[k], w);
       if(CHECK && soft)
         {
 #pragma unroll 1
-          for(int u = 0; u < kUnroll; u++)
+          for(int u = 0; u < U; u++)
             {
               const V4<R> eu = LP[j + u];
               const R hu     = LH[j + u];
@@ -613,7 +623,7 @@ __device__ __forceinline__ void push(List<R> &L, bool keep, const V4<R> e, R h, 
 }
 
 template <bool PERIODIC, bool POT, int TPL, bool EWALD = false, typename R = float>
-__global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS : 3) k_walk32(const double4 *__restrict__ g_sm, const float4 *__restrict__ g_rel,
+__global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? (TPL == 2 ? GG_W32_MINBLOCKS2 : GG_W32_MINBLOCKS) : 3) k_walk32(const double4 *__restrict__ g_sm, const float4 *__restrict__ g_rel,
                                                         const int4 *__restrict__ g_kids, const double4 *__restrict__ g_pm,
                                                         const uint8_t *__restrict__ g_pst, const double4 *__restrict__ tpm,
                                                         const uint8_t *__restrict__ tst, const float *__restrict__ oldacc,
@@ -935,17 +945,20 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? GG_W32_MINBLOCKS
           push<R, PERIODIC>(L, action == 1 && !split, entry, (R)hj, ent_d2, fmaxf(h_grp, hj), ex, ey, ez, w, lt_mask);
           t_next = 0;
           t_end  = __ballot_sync(0xffffffffu, action == 1 && split) ? w.nsoft : 0;
-          // particles of opened nodes: pending rounds
-          const int npx = (action == 2) ? np : 0;
-          pinc          = wscan_incl(npx, lane);
-          ptot          = __shfl_sync(0xffffffffu, pinc, 31);
-          pexc          = pinc - npx;
-          q0            = 0;
+          // particles (pending rounds) and node children of opened nodes: one scan of both counts
+          // (each below 16, particles in the low half-word)
+          const int npx  = (action == 2) ? np : 0;
+          const int ncx  = (action == 2) ? nc : 0;
+          const int both = wscan_incl(npx | (ncx << 16), lane);
+          const int tot  = __shfl_sync(0xffffffffu, both, 31);
+          pinc           = both & 0xffff;
+          ptot           = tot & 0xffff;
+          pexc           = pinc - npx;
+          q0             = 0;
           WALK_STAT(2, ptot);
           // node children of opened nodes -> stack (contiguous in breadth-first order)
-          const int ncx  = (action == 2) ? nc : 0;
-          const int cinc = wscan_incl(ncx, lane);
-          const int ctot = __shfl_sync(0xffffffffu, cinc, 31);
+          const int cinc = both >> 16;
+          const int ctot = tot >> 16;
           if(sp + ctot <= kStackCap)
             {
               const int cb = sp + cinc - ncx;
@@ -1305,8 +1318,10 @@ cudaError_t walk32_prepare(gpugrav_ctx *c, const WalkConst &wc)
   const bool fp64     = c->prm.precision == GPUGRAV_PREC_FP64_GROUP;
   if(fp64 && wc.ewald)
     return cudaErrorNotSupported;
-  Walk32Kernel kern = fp64 ? (periodic ? (pot ? k_walk32<true, true, 1, false, double> : k_walk32<true, false, 1, false, double>)
-                                       : (pot ? k_walk32<false, true, 1, false, double> : k_walk32<false, false, 1, false, double>))
+  Walk32Kernel kern = fp64 ? (tpl == 2 ? (periodic ? (pot ? k_walk32<true, true, 2, false, double> : k_walk32<true, false, 2, false, double>)
+                                                    : (pot ? k_walk32<false, true, 2, false, double> : k_walk32<false, false, 2, false, double>))
+                                      : (periodic ? (pot ? k_walk32<true, true, 1, false, double> : k_walk32<true, false, 1, false, double>)
+                                                  : (pot ? k_walk32<false, true, 1, false, double> : k_walk32<false, false, 1, false, double>)))
                     : wc.ewald ? (pot ? k_walk32<false, true, 1, true> : k_walk32<false, false, 1, true>)
                       : tpl == 2 ? (periodic ? (pot ? k_walk32<true, true, 2> : k_walk32<true, false, 2>)
                                              : (pot ? k_walk32<false, true, 2> : k_walk32<false, false, 2>))

@@ -64,7 +64,7 @@ FLOPS_PER_INTERACTION = 23.0  # convention of the path's roofline
 # in L2)
 WALK32_DRAM_BYTES_PER_PARTICLE = 363.5e6 / (1 << 21)
 # ErrTolForceAcc of the per-target FP64 walk in the precision ablation: the value at which its RMS
-# error on the zoom box matches the FP32 walk's at 5e-5 (8.1e-4 against 9.3e-4)
+# error on the zoom box is at most the FP32 walk's at 6e-5 (8.2e-4 against 9.4e-4)
 ABLATION_FP64_ALPHA = 2e-5
 
 
@@ -794,9 +794,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp32")
-    ap.add_argument("--err-tol-force-acc", type=float, default=5e-5,
-                    help="ErrTolForceAcc of the timed relative-criterion steps; 5e-5 keeps the FP32 walk's RMS force "
-                         "error below 1e-3 on the zoom box (the metric's accuracy bar)")
+    ap.add_argument("--err-tol-force-acc", type=float, default=6e-5,
+                    help="ErrTolForceAcc of the timed relative-criterion steps; 6e-5 keeps the FP32 walk's RMS force "
+                         "error below 1e-3 on the zoom box (the metric's accuracy bar: 9.4e-4)")
     ap.add_argument("--log2-half", type=int, default=23, help="log2 of each species' count (23 -> N=2^24)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
