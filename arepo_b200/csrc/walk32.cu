@@ -41,14 +41,14 @@ namespace
 constexpr int kWarps   = GG_W32_WARPS;    // warps per block
 constexpr int kEvalAt  = GG_W32_EVAL_AT;  // evaluate once this many entries are queued
 #ifndef GG_W32_MINBLOCKS
-#define GG_W32_MINBLOCKS 6  // blocks per SM the register budget is sized for (80 registers a thread, 31 KB of shared memory a block)
+#define GG_W32_MINBLOCKS 7  // blocks per SM the register budget is sized for (72 registers a thread, 31 KB of shared memory a block)
 #endif
-// two targets per lane: fewer entries in flight, 96 registers (5 blocks per SM)
+// two targets per lane: fewer entries in flight, 80 registers (6 blocks per SM, 35 KB of shared memory a block)
 #ifndef GG_W32_UNROLL2
 #define GG_W32_UNROLL2 4
 #endif
 #ifndef GG_W32_MINBLOCKS2
-#define GG_W32_MINBLOCKS2 5
+#define GG_W32_MINBLOCKS2 6
 #endif
 // list entries in flight per lane in the evaluation loop
 template <int TPL>
@@ -622,6 +622,14 @@ __device__ __forceinline__ void push(List<R> &L, bool keep, const V4<R> e, R h, 
   L.nn += __popc(kn);
 }
 
+// A warp's group: centre (FP64), half extents, smallest and (with margin) largest target softening,
+// smallest ErrTolForceAcc x |OldAcc|, and the per-target vote's squared size bound.
+struct GroupSh
+{
+  double gx, gy, gz;
+  float ex, ey, ez, h_min, h_grp, aold_min, vote_r2;
+};
+
 template <bool PERIODIC, bool POT, int TPL, bool EWALD = false, typename R = float>
 __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? (TPL == 2 ? GG_W32_MINBLOCKS2 : GG_W32_MINBLOCKS) : 3) k_walk32(const double4 *__restrict__ g_sm, const float4 *__restrict__ g_rel,
                                                         const int4 *__restrict__ g_kids, const double4 *__restrict__ g_pm,
@@ -646,6 +654,7 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? (TPL == 2 ? GG_W
   __shared__ double dsum_sh[kWarps][4 * TPL][32];
   __shared__ float aold_sh[kWarps][32 * TPL];
   __shared__ unsigned long long total_sh[kWarps];
+  __shared__ GroupSh group_sh[kWarps];
   static_assert(kW32Bytes<R> % 4 == 0, "constants copied in 4-byte words");
   for(int t = threadIdx.x; t < kW32Bytes<R> / 4; t += blockDim.x)
     ((int *)w_raw)[t] = ((const int *)wcp)[t];
@@ -706,17 +715,28 @@ __global__ void __launch_bounds__(32 * kWarps, sizeof(R) == 4 ? (TPL == 2 ? GG_W
         }
       // group box (FP64), centre g, half extent (rounded up)
       mnx = wmin(mnx), mxx = wmax(mxx), mny = wmin(mny), mxy = wmax(mxy), mnz = wmin(mnz), mxz = wmax(mxz);
-      const double gx = 0.5 * (mnx + mxx), gy = 0.5 * (mny + mxy), gz = 0.5 * (mnz + mxz);
-      const float ex = (float)(0.5 * (mxx - mnx)) * 1.000001f, ey = (float)(0.5 * (mxy - mny)) * 1.000001f,
-                  ez = (float)(0.5 * (mxz - mnz)) * 1.000001f;
-      const float h_min    = wminf(hmin_l);
-      // an entry farther than max(h_grp, h_j) from the group box is outside the softening length of
-      // every target (the margin covers the rounding of the FP32 separations)
-      const float h_grp    = wmaxf(hmax_l) * 1.001f;
-      const float aold_min = wminf(amin_l);
-      // box side squared over kVote^2: a node smaller than this and closer than it gets the per-target vote
-      const float side     = 2.0f * fmaxf(ex, fmaxf(ey, ez));
-      const float vote_r2  = side * side * (1.0f / (kVote * kVote));
+      {
+        GroupSh g;
+        g.gx = 0.5 * (mnx + mxx), g.gy = 0.5 * (mny + mxy), g.gz = 0.5 * (mnz + mxz);
+        g.ex = (float)(0.5 * (mxx - mnx)) * 1.000001f, g.ey = (float)(0.5 * (mxy - mny)) * 1.000001f,
+        g.ez = (float)(0.5 * (mxz - mnz)) * 1.000001f;
+        g.h_min = wminf(hmin_l);
+        // an entry farther than max(h_grp, h_j) from the group box is outside the softening length of
+        // every target (the margin covers the rounding of the FP32 separations)
+        g.h_grp    = wmaxf(hmax_l) * 1.001f;
+        g.aold_min = wminf(amin_l);
+        // box side squared over kVote^2: a node smaller than this and closer than it gets the per-target vote
+        const float side = 2.0f * fmaxf(g.ex, fmaxf(g.ey, g.ez));
+        g.vote_r2        = side * side * (1.0f / (kVote * kVote));
+        if(lane == 0)
+          group_sh[warp] = g;
+      }
+      __syncwarp();
+      // the group's constants are read from shared memory where they are used (out of registers)
+      const GroupSh &gs = group_sh[warp];
+      const double &gx = gs.gx, &gy = gs.gy, &gz = gs.gz;
+      const float &ex = gs.ex, &ey = gs.ey, &ez = gs.ez, &h_min = gs.h_min, &h_grp = gs.h_grp, &aold_min = gs.aold_min,
+                  &vote_r2 = gs.vote_r2;
       Tgt<R> T[TPL];
 #pragma unroll
       for(int k = 0; k < TPL; k++)
