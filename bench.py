@@ -59,10 +59,10 @@ METRIC = "tree-gravity particles/s at N=2^24 (RMS force err ≤1e-3); serving p5
 UNIT = "particles/s"
 FLOPS_PER_INTERACTION = 23.0  # convention of the path's roofline
 # DRAM bytes (read + write) of one FP32 walk launch per particle: ncu capture of the zoom box at
-# N=2^21 (dram__bytes_read.sum + dram__bytes_write.sum = 287.5 MB + 79.1 MB), scaled by the
+# N=2^21 (dram__bytes_read.sum + dram__bytes_write.sum = 298.9 MB + 84.3 MB), scaled by the
 # particle count (the walk reads the tree and the particles once from DRAM; everything else hits
 # in L2)
-WALK32_DRAM_BYTES_PER_PARTICLE = 366.5e6 / (1 << 21)
+WALK32_DRAM_BYTES_PER_PARTICLE = 383.2e6 / (1 << 21)
 # ErrTolForceAcc of the per-target FP64 walk in the precision ablation: the value at which its RMS
 # error on the zoom box is at most the FP32 walk's at 6e-5 (8.2e-4 against 9.4e-4)
 ABLATION_FP64_ALPHA = 2e-5
