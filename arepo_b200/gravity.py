@@ -101,8 +101,19 @@ class GravityTree:
             cost = np.ascontiguousarray(cost, np.float32)
         self._check(self.lib.gpugrav_set_target_slice_cost(self._ctx, slice_, nslices, n, L.ptr(cost), mem))
 
+    # cudaStreamLegacy: the legacy default stream as an explicit handle (cuda_runtime_api.h)
+    _CUDA_STREAM_LEGACY = 0x1
+
     def set_stream(self, stream_handle: int | None):
-        self._check(self.lib.gpugrav_set_stream(self._ctx, C.c_void_p(stream_handle) if stream_handle else None))
+        """Run the context's work on `stream_handle` (a cudaStream_t as an int, e.g. a torch stream's
+        `cuda_stream`); None: the context's own stream.  0 is the legacy default stream (torch's default
+        stream), which the C ABI takes as cudaStreamLegacy (NULL there means the context's own stream,
+        which does not order against the caller's work)."""
+        if stream_handle is None:
+            h = None
+        else:
+            h = C.c_void_p(stream_handle if stream_handle != 0 else self._CUDA_STREAM_LEGACY)
+        self._check(self.lib.gpugrav_set_stream(self._ctx, h))
 
     def synchronize(self):
         self._check(self.lib.gpugrav_synchronize(self._ctx))

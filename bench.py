@@ -445,6 +445,10 @@ def sharded_arm(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    # stdout carries the JSON line only: what the libraries print (NCCL's version banner) goes to stderr
+    sys.stdout.flush()
+    stdout_fd = os.dup(1)
+    os.dup2(2, 1)
     os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
     os.environ.setdefault("MASTER_PORT", "29541")
     os.environ.setdefault("RANK", str(rank))
@@ -548,6 +552,9 @@ def sharded_arm(args):
     sg.close()
     dist.barrier()
     dist.destroy_process_group()
+    sys.stdout.flush()
+    os.dup2(stdout_fd, 1)
+    os.close(stdout_fd)
     if line is not None:
         print(json.dumps(line), flush=True)
     return 0

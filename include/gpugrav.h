@@ -165,7 +165,8 @@ int32_t gpugrav_abi_version(void);
 int32_t gpugrav_create(gpugrav_ctx **ctx, int32_t device, const gpugrav_params *params);
 int32_t gpugrav_destroy(gpugrav_ctx *ctx);
 int32_t gpugrav_set_params(gpugrav_ctx *ctx, const gpugrav_params *params);
-/* Run all library work on a caller-owned cudaStream_t (NULL: the context's own stream). */
+/* Run all library work on a caller-owned cudaStream_t (NULL: the context's own non-blocking stream,
+ * which does not order against the caller's work; the legacy default stream is cudaStreamLegacy). */
 int32_t gpugrav_set_stream(gpugrav_ctx *ctx, void *cuda_stream);
 int32_t gpugrav_synchronize(gpugrav_ctx *ctx);
 
