@@ -265,6 +265,7 @@ def reference_arm(args):
 SERVE_NMIN, SERVE_NMAX = 1000, 1000000
 SERVE_EPS, SERVE_K, SERVE_DT = 0.02, 16, 0.005
 SERVE_BUDGET = 120e9
+SERVE_CLASS_REQUESTS = 16  # requests per size decade in the per-class comparison
 
 
 def serving_stream(count: int, seed: int = 1005):
@@ -406,6 +407,22 @@ def serving_leg(args, device):
     log(f"serving: serial {serial['requests_per_s']:.2f} req/s")
     plain = run_plain_serial(systems, cmp_ids, device)
     log(f"serving: plain API serial {plain['requests_per_s']:.2f} req/s")
+    # the same comparison per decade of system size: where continuous batching pays
+    by_size = []
+    for lo_n, hi_n in ((SERVE_NMIN, 10 * SERVE_NMIN), (10 * SERVE_NMIN, 100 * SERVE_NMIN), (100 * SERVE_NMIN, SERVE_NMAX + 1)):
+        ids = np.nonzero((ns >= lo_n) & (ns < hi_n))[0][:SERVE_CLASS_REQUESTS]
+        if len(ids) == 0:
+            continue
+        b = run_stream(systems, ids, None, 4096, device, pool)
+        s1 = run_stream(systems, ids, None, 1, device, pool)
+        by_size.append({"n_range": [int(lo_n), int(hi_n)], "requests": int(len(ids)),
+                        "particles": int(ns[ids].sum()),
+                        "batched_requests_per_s": b["requests_per_s"], "serial_requests_per_s": s1["requests_per_s"],
+                        "batched_particle_steps_per_s": b["particle_steps_per_s"],
+                        "serial_particle_steps_per_s": s1["particle_steps_per_s"],
+                        "batched_latency_p99_s": b["latency_p99_s"], "serial_latency_p99_s": s1["latency_p99_s"],
+                        "throughput_ratio": b["particle_steps_per_s"] / s1["particle_steps_per_s"]})
+        log(f"serving: N in [{lo_n}, {hi_n}): batched/serial {by_size[-1]['throughput_ratio']:.2f}")
     rate = args.serve_load * batched["requests_per_s"]
     arr = np.cumsum(np.random.default_rng(1006).exponential(1.0 / rate, len(ns)))
     poisson = run_stream(systems, np.arange(len(ns)), arr, 4096, device, pool)
@@ -423,6 +440,7 @@ def serving_leg(args, device):
                     "serial_note": "serial_max_systems_1: the serving loop admitting one request at a time (device-"
                                    "resident particles, the same kernels); serial_plain_api: one gpugrav_compute call "
                                    "per force evaluation on host arrays, kick/drift on the host"},
+        "by_size_class": by_size,
         "poisson": dict(poisson, rate_per_s=rate, load=args.serve_load),
         "clock": "host wall clock of the serving loop (uploads, ticks, downloads included)",
     }
