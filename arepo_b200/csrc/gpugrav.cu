@@ -305,7 +305,7 @@ int32_t gpugrav_create(gpugrav_ctx **out, int32_t device, const gpugrav_params *
   c->device = device;
   c->prm    = *p;
   if(const char *e = getenv("GPUGRAV_WALK32_TPL"))
-    c->walk32_tpl = atoi(e) == 1 ? 1 : 2;
+    c->walk32_tpl = atoi(e) == 1 ? 1 : atoi(e) == 2 ? 2 : 0;
   if(const char *e = getenv("GPUGRAV_GROUP_SLACK"))
     c->group_slack = atoi(e);
   if(const char *e = getenv("GPUGRAV_PROFILE"))

@@ -242,7 +242,7 @@ struct gpugrav_ctx
   void *w32_kernel   = nullptr;
   int32_t w32_blocks = 0;
   bool want_pot       = true;  // potential requested by the current walk call
-  int walk32_tpl      = 2;     // targets per lane of the FP32 walk (1 or 2; GPUGRAV_WALK32_TPL)
+  int walk32_tpl      = 0;     // targets per lane of the group walk: 0 auto, 1 or 2 (GPUGRAV_WALK32_TPL)
   gg::DevBuf acc_s, pot_s, nint_s, oldacc_s, oldacc_in;  // per target (sorted), inputs
   gg::DevBuf out_acc, out_pot, out_nint;      // caller order staging for host copies
   gg::DevBuf scratch;                         // reductions
@@ -291,13 +291,16 @@ cudaError_t direct_stage(gpugrav_ctx *c, const WalkConst &wc, int64_t nt, const 
 cudaError_t gravity_direct_stage(gpugrav_ctx *c, int64_t n, const double *d_pos, const double *d_mass, const uint8_t *d_st,
                                  double *d_acc, double *d_pot, int32_t *d_nint, int *d_flag);
 void make_walk_const(const gpugrav_params &p, WalkConst *wc);
-// targets per lane of the group walk: 2 (groups of 64 targets; GPUGRAV_WALK32_TPL=1 asks for 32) for
-// the TreePM or isolated group walk of one system (FP32, or its FP64 form), else 1
+// targets per lane of the group walk (FP32, or its FP64 form; TreePM or isolated): by default 2 (groups
+// of 64 targets) for one system and 1 for the serving loop's batched systems; GPUGRAV_WALK32_TPL=1 or 2
+// forces either.  The Ewald walk and the per-target walk: 1.
 inline int walk32_tpl(const gpugrav_ctx *c)
 {
   const bool ewald = c->prm.periodic && !(c->prm.asmth > 0);
   const bool group = c->prm.precision == GPUGRAV_PREC_FP32 || c->prm.precision == GPUGRAV_PREC_FP64_GROUP;
-  return (c->walk32_tpl == 1 || c->multi || ewald || !group) ? 1 : 2;
+  if(ewald || !group || c->walk32_tpl == 1)
+    return 1;
+  return (c->walk32_tpl == 2 || !c->multi) ? 2 : 1;
 }
 // GPUGRAV_OK or GPUGRAV_ERR_INVALID: ABI version, softening table (finite, >= 0, zero end entry),
 // box size, TreePM split (asmth, rcut, rcut_cells > 0 unless asmth == 0), tolerances, flags
