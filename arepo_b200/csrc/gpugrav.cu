@@ -308,6 +308,8 @@ int32_t gpugrav_create(gpugrav_ctx **out, int32_t device, const gpugrav_params *
     c->walk32_tpl = atoi(e) == 1 ? 1 : atoi(e) == 2 ? 2 : 0;
   if(const char *e = getenv("GPUGRAV_GROUP_SLACK"))
     c->group_slack = atoi(e);
+  if(const char *e = getenv("GPUGRAV_ACTIVE_GROUP_SLACK"))
+    c->active_slack = atoi(e);
   if(const char *e = getenv("GPUGRAV_PROFILE"))
     c->profile = atoi(e) != 0;
   DeviceGuard g(device);
@@ -349,7 +351,7 @@ int32_t gpugrav_destroy(gpugrav_ctx *c)
                         &c->n_next, &c->n_dfs, &c->n_first, &c->p_next, &c->p_father, &c->p_dfs, &c->depth_hist,
                         &c->depth_order, &c->w_sm, &c->w_cl, &c->w_link, &c->g_key, &c->g_key_alt, &c->g_val, &c->g_val_alt, &c->g_bfs, &c->g_np, &c->g_poff, &c->g_sm, &c->g_rel, &c->g_kids, &c->g_pm, &c->g_pst, &c->g_stack, &c->acc_s, &c->pot_s,
                         &c->nint_s, &c->oldacc_s, &c->oldacc_in, &c->out_acc, &c->out_pot, &c->out_nint, &c->scratch,
-                        &c->g_groups, &c->g_ngroups, &c->g_gpd, &c->g_gseg, &c->g_gflag, &c->g_gid, &c->m_sys, &c->m_doms,
+                        &c->g_groups, &c->g_ngroups, &c->g_gpd, &c->g_gseg, &c->g_gflag, &c->g_gid, &c->t_cd, &c->t_pd, &c->m_sys, &c->m_doms,
                         &c->pm_pos, &c->pm_mass, &c->pm_acc, &c->pm_pot, &c->ewd, &c->ewd32, &c->n_mpt, &c->w_mpt,
                         &c->g_mpt, &c->iperm, &c->t_in, &c->t_pos, &c->t_pos_alt, &c->t_idx, &c->t_idx_alt,
                         &c->cost_in, &c->cost_u, &c->cost_p, &c->slice_rng};

@@ -212,6 +212,7 @@ struct gpugrav_ctx
   gg::DevBuf g_stack;                         // per-warp traversal stacks
   gg::DevBuf g_groups, g_ngroups;             // walk groups (first, count, root, criterion), their count
   gg::DevBuf g_gpd, g_gseg, g_gflag, g_gid;   // group construction scratch
+  gg::DevBuf t_cd, t_pd;                      // active list: pair depths of consecutive targets, their cell depths
   int32_t slice = 0, nslices = 1;             // target slice of the walks (gpugrav_set_target_slice)
   // active targets of the current walk (gpugrav_walk_targets): sorted particle positions in key order
   // (t_pos_alt) and their places in the caller's list (t_idx_alt); w_tlist is null for a walk of every particle
@@ -233,6 +234,7 @@ struct gpugrav_ctx
   int32_t pm_grid = 0, pm_plan_f = 0, pm_plan_b = 0;
   gg::DevBuf pm_rho, pm_rhok, pm_pos, pm_mass, pm_acc, pm_pot, pm_tab;
   int group_slack = 99;                       // group cuts between cells (< 64) or key order only (GPUGRAV_GROUP_SLACK)
+  int active_slack = 2;                       // the same for groups of an active list (GPUGRAV_ACTIVE_GROUP_SLACK)
   bool layout32_valid = false;
   // several independent systems in one build (serving): system of each sorted particle, domain of
   // each system (walk groups never span two systems)
@@ -251,6 +253,14 @@ struct gpugrav_ctx
   cudaEvent_t ev[20] = {};
   gpugrav_timings timings{};
 };
+
+// depth of the deepest tree cell holding two particles, from their integer positions (52 bits per
+// axis below the domain cube; 52 when they coincide)
+__device__ __forceinline__ int common_depth(uint64_t ax, uint64_t ay, uint64_t az, uint64_t bx, uint64_t by, uint64_t bz)
+{
+  uint64_t d = (ax ^ bx) | (ay ^ by) | (az ^ bz);
+  return d == 0 ? 52 : (__clzll((long long)d) - 12);
+}
 
 namespace gg
 {

@@ -55,16 +55,6 @@ __global__ void k_target_dups(int64_t nt, const uint32_t *__restrict__ pos, int 
       atomicOr(flag, 2);
 }
 
-// FP32 walk groups over the active list: `cap` consecutive entries each (one system, root 0)
-__global__ void k_grp_active(int64_t nt, int cap, int4 *__restrict__ groups, int *__restrict__ ngroups)
-{
-  const int64_t ng = (nt + cap - 1) / cap;
-  for(int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ng; g += (int64_t)gridDim.x * blockDim.x)
-    groups[g] = make_int4((int)(g * cap), (int)((nt - g * cap) < cap ? (nt - g * cap) : cap), 0, -1);
-  if(blockIdx.x == 0 && threadIdx.x == 0)
-    *ngroups = (int)ng;
-}
-
 // results of the active list back to the caller's list order; entries outside [a, b) of the
 // active list (another rank's target slice) are written as zero
 __global__ void k_scatter_targets(int64_t nt, const uint32_t *__restrict__ tpos, const uint32_t *__restrict__ tidx, int64_t a,
@@ -117,13 +107,6 @@ cudaError_t targets_stage(gpugrav_ctx *c, int64_t nt, const int32_t *d_targets, 
   GG_TRY(cudaMemcpyAsync(flags, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
   GG_TRY(cudaStreamSynchronize(st));
   return cudaSuccess;
-}
-
-cudaError_t groups_active_stage(gpugrav_ctx *c, int64_t nt, int cap)
-{
-  GG_TRY(c->g_groups.ensure(((nt + cap - 1) / cap + 1) * sizeof(int4)));
-  k_grp_active<<<grid_for((nt + cap - 1) / cap, 256), 256, 0, c->stream>>>(nt, cap, c->g_groups.as<int4>(), c->g_ngroups.as<int>());
-  return cudaGetLastError();
 }
 
 cudaError_t targets_scatter(gpugrav_ctx *c, int64_t nt, int64_t a, int64_t b, double *acc, double *pot, int32_t *nint)

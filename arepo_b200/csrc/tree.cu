@@ -39,12 +39,6 @@ struct SkelInfo
   int32_t max_top_depth;
 };
 
-__device__ __forceinline__ int common_depth(uint64_t ax, uint64_t ay, uint64_t az, uint64_t bx, uint64_t by, uint64_t bz)
-{
-  uint64_t d = (ax ^ bx) | (ay ^ by) | (az ^ bz);
-  return d == 0 ? 52 : (__clzll((long long)d) - 12);
-}
-
 __device__ __forceinline__ int morton_slot(uint64_t x, uint64_t y, uint64_t z, int depth)
 {
   // child index inside a node of depth (depth-1): bits 52-depth, x | y<<1 | z<<2 (src/gravity/forcetree.c:854-855)
