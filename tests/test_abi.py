@@ -80,3 +80,27 @@ def test_null_context_calls_fail_cleanly(lib):
     assert lib.gpugrav_destroy(None) == L.ERR_INVALID
     assert lib.gpugrav_build(None, None, 0) == L.ERR_INVALID
     assert lib.gpugrav_walk(None, None, None, None, None, 0) == L.ERR_INVALID
+
+
+def test_set_stream_handles():
+    """GravityTree.set_stream: None asks for the context's own stream (NULL); torch's default stream
+    (handle 0) is the legacy default stream, passed as cudaStreamLegacy so that the library's work is
+    ordered after the caller's; other handles pass through.  A stand-in library records the calls."""
+    import ctypes as C
+
+    from arepo_b200.gravity import GravityTree
+
+    seen = []
+
+    class FakeLib:
+        def gpugrav_set_stream(self, ctx, h):
+            seen.append(None if h is None else h.value)
+            return 0
+
+    t = object.__new__(GravityTree)
+    t.lib, t._ctx = FakeLib(), C.c_void_p(1)
+    t._check = lambda s: None
+    t.set_stream(None)
+    t.set_stream(0)
+    t.set_stream(0x7F00)
+    assert seen == [None, 0x1, 0x7F00]
